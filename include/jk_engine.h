@@ -1,0 +1,91 @@
+/* jk_engine.h — C ABI of the B200 J/K Fock-build engine.
+ *
+ * Drop-in for the two-electron part of molecular2's Fock / IntegralEngine
+ * (rashaw1/molecular2).  Every entry point below names the reference
+ * interface it replaces (path:line inside molecular2).  Plain pointers and
+ * sizes only: no C++ or torch types cross this boundary.
+ *
+ * Conventions
+ *  - Matrices are column-major like molecular2's `Matrix` (Eigen::MatrixXd,
+ *    inc/eigen_wrapper.hpp:8).  D, J, K, S, T, V are symmetric n x n; Cocc is
+ *    n x nocc column-major.
+ *  - Basis functions follow shell order; inside a shell libint2's order:
+ *    Cartesian x^a y^b z^c for a = l..0, b = l-a..0; pure (spherical) shells
+ *    m = -l..l.  Pure applies to shells with l >= 2 whose `pure` flag is set.
+ *  - `coefs` are the coefficients as printed in the basis library (for
+ *    normalised primitives); the engine normalises them as libint2::Shell
+ *    does (src/basis.cpp:49-61 constructs those shells).
+ *  - Coordinates are bohr.
+ *  - Return value: 0 on success, else a JK_ERR_* code; jk_last_error() gives
+ *    the message.  Nothing aborts, throws across the boundary or traps on the
+ *    device (molecular2 throws Error(code,msg), inc/error.hpp:25-29).
+ *  - One engine = one CUDA device + one stream.  Calls on one engine are not
+ *    re-entrant; different engines are independent.
+ *  - `*_device` variants take device pointers and a cudaStream_t (as void*,
+ *    NULL = the engine's stream) and do not synchronise the host.
+ */
+#ifndef M2_JK_ENGINE_H
+#define M2_JK_ENGINE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  JK_OK = 0,
+  JK_ERR_ARG = 1,         /* bad argument (null pointer, size, unsupported l) */
+  JK_ERR_CUDA = 2,        /* CUDA / cuBLAS / cuSOLVER failure */
+  JK_ERR_NOT_PD = 3,      /* fitting metric (P|Q) not positive definite */
+  JK_ERR_STATE = 4,       /* call order (e.g. jk_df before jk_df_setup) */
+  JK_ERR_NOMEM = 5,       /* device allocation failed */
+  JK_ERR_NOT_CONVERGED = 6
+};
+
+/* Struct-of-arrays Gaussian basis.  Replaces std::vector<libint2::Shell>
+ * built by Basis::addShell (src/basis.cpp:33-66). */
+typedef struct jk_basis {
+  int nshell;
+  const int* l;          /* angular momentum per shell */
+  const int* nprim;      /* primitives per shell */
+  const int* prim_off;   /* offset of the shell's primitives in exps/coefs */
+  const double* exps;    /* exponents */
+  const double* coefs;   /* contraction coefficients (as printed) */
+  const double* xyz;     /* 3 * nshell centre coordinates, bohr */
+  const int* pure;       /* per shell: 1 = spherical for l >= 2 (NULL: all Cartesian) */
+  const int* atom;       /* per shell: owning atom (NULL allowed when no gradient is needed) */
+} jk_basis;
+
+typedef struct jk_engine jk_engine;
+
+/* Create an engine for an orbital basis and (optionally, NULL) a fitting
+ * basis; natom point charges Z at atom_xyz (3*natom) for one-body and
+ * gradient terms.  Computes the Schwarz bounds of all shell pairs.
+ * Replaces the IntegralEngine constructor's prescreen step
+ * (src/integrals.cpp:42-124, compute_schwarz_ints at :95). */
+int jk_create(const jk_basis* obs, const jk_basis* aux, int natom, const double* atom_xyz, const double* Z,
+              int device, jk_engine** out);
+void jk_destroy(jk_engine* e);
+const char* jk_last_error(const jk_engine* e);
+
+/* Basis sizes: n (orbital), naux (fitting, 0 if none), nshell (orbital). */
+int jk_sizes(const jk_engine* e, int* n, int* naux, int* nshell);
+
+/* Schwarz matrix Q(s1,s2) = sqrt(max_i |(ab|ab)_ii|), nshell x nshell.
+ * Replaces IntegralEngine::compute_schwarz_ints (src/integrals.cpp:472-513). */
+int jk_schwarz(const jk_engine* e, double* Q);
+
+/* Integral-direct J[D] and K[D] (both w.r.t. the full D passed in, scaled by
+ * `multiplier`), FP64, Schwarz x density screening at `precision`:
+ * Fock::formJKdirect(Schwarz, D, multiplier) (src/fockbuild.cpp:64-164);
+ * the caller forms jkints = J - 0.5 K as :163 does. Host pointers. */
+int jk_direct(jk_engine* e, const double* D, double precision, double multiplier, double* J, double* K);
+int jk_direct_device(jk_engine* e, const double* dD, double precision, double multiplier, double* dJ,
+                     double* dK, void* stream);
+
+/* Number of shell quartets the last direct build evaluated. */
+long long jk_last_quartets(const jk_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,132 @@
+// Internal engine state shared by the .cu translation units (not part of the C ABI).
+#pragma once
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/jk_engine.h"
+
+namespace m2 {
+
+constexpr int MAX_L_OBS = 2;  // orbital shells up to d
+constexpr int MAX_L_AUX = 3;  // fitting shells up to f
+constexpr int NPAIRCLASS = (MAX_L_OBS + 1) * (MAX_L_OBS + 2) / 2;
+
+inline int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }  // la >= lb
+
+// Host copy of a normalised basis in the engine's layout.
+struct HostBasis {
+  int nshell = 0;
+  std::vector<int> l, nprim, prim_off, atom, pure;
+  std::vector<double> exps, coefs, xyz;   // coefs normalised (libint2 Shell semantics)
+  std::vector<int> off_final, off_cart;   // per shell (+1 entry): function offsets
+  int n_final = 0, n_cart = 0;
+  int max_l = 0;
+};
+
+// Device array with RAII.
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    if (count == n && p) return cudaSuccess;
+    reset();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    return e;
+  }
+  cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
+    cudaError_t e = alloc(v.size());
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+};
+
+// Shell data on the device (one basis).
+struct DevBasis {
+  DevBuf<int> l, cart_off, final_off, nprim, prim_off, atom, pure;
+  DevBuf<double> x, y, z, exps, coefs;
+  DevBuf<double> sph;       // packed solid-harmonic blocks, l = 0..SPH_LMAX (sph_off)
+  DevBuf<int> cart_shell, cart_comp, final_shell, final_comp;  // per function
+};
+
+// Shell pairs of one angular class (la >= lb), sorted by Schwarz bound (descending).
+struct PairClassHost {
+  int la = 0, lb = 0;
+  std::vector<int> sa, sb, prim_off, nprim;
+  std::vector<double> Q;
+};
+struct PairClassDev {
+  int la = 0, lb = 0, npair = 0;
+  DevBuf<int> sa, sb, prim_off, nprim;
+  DevBuf<double> Q;
+};
+
+struct DFState {
+  bool ready = false;
+  int naux = 0, npair_bf = 0;
+  DevBuf<double> B64;      // [x][K][y] unpacked, FP64
+  DevBuf<float> B32;       // same layout, FP32 copy for the mixed path
+  DevBuf<double> L;        // Cholesky factor of the metric (naux x naux, col-major)
+};
+
+}  // namespace m2
+
+struct jk_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t cublas = nullptr;
+  cusolverDnHandle_t cusolver = nullptr;
+  std::string err;
+
+  int natom = 0;
+  std::vector<double> atom_xyz, Z;
+
+  m2::HostBasis obs, aux;
+  bool has_aux = false;
+  m2::DevBasis dobs, daux;
+
+  // shell pairs (orbital basis)
+  m2::PairClassDev pcls[m2::NPAIRCLASS];
+  m2::DevBuf<double> pp_p, pp_x, pp_y, pp_z, pp_K;  // primitive pairs
+  std::vector<double> schwarz_host;                  // nshell x nshell, row-major (symmetric)
+  m2::DevBuf<double> schwarz_dev;                    // nshell x nshell
+  double Qmax = 0.0;
+
+  m2::DevBuf<double> boys;                           // Boys table
+
+  // scratch for J/K builds
+  m2::DevBuf<double> Dcart, Jcart, Kcart, Dnorm, Dmax, Dfinal, Jfinal, Kfinal;
+  m2::DFState df;
+  long long last_quartets = 0;
+};
+
+namespace m2 {
+// engine.cu
+int set_error(jk_engine* e, int code, const std::string& msg);
+int check_cuda(jk_engine* e, cudaError_t st, const char* what);
+int build_basis(const jk_basis* b, bool allow_pure, int lmax, HostBasis& out, std::string& err);
+int upload_basis(jk_engine* e, const HostBasis& hb, DevBasis& db);
+// jk_direct.cu
+int build_pairs(jk_engine* e);
+int direct_jk_device(jk_engine* e, const double* dD, double precision, double mult, double* dJ, double* dK,
+                     cudaStream_t s);
+// transforms (cart <-> final) and norms
+void launch_final_to_cart(const jk_engine* e, const double* Dfinal, double* Dcart, cudaStream_t s);
+void launch_cart_to_final_sym(const jk_engine* e, const double* Xcart, double scale, double* Xfinal, cudaStream_t s);
+void launch_shell_norms(const jk_engine* e, const double* Dfinal, double* Dnorm, double* Dmax, cudaStream_t s);
+}  // namespace m2

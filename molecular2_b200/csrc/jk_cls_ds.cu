@@ -1,0 +1,13 @@
+// Kernel instantiations of the direct J/K build, bra class ds.
+// Split across translation units only so that nvcc compiles them in parallel.
+#include "jk_kernels.cuh"
+
+namespace m2 {
+void launch_jk_bra_ds(int B, const JKParams& P, dim3 grid, cudaStream_t s) {
+  if (B == 0) k_jk_direct<2, 0, 0, 0><<<grid, 128, 0, s>>>(P);
+  if (B == 1) k_jk_direct<2, 0, 1, 0><<<grid, 128, 0, s>>>(P);
+  if (B == 2) k_jk_direct<2, 0, 1, 1><<<grid, 128, 0, s>>>(P);
+  if (B == 3) k_jk_direct<2, 0, 2, 0><<<grid, 128, 0, s>>>(P);
+}
+
+}  // namespace m2

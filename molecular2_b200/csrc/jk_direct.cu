@@ -1,0 +1,243 @@
+// Integral-direct J/K build (FP64) — the B200 replacement for
+// Fock::formJKdirect (molecular2 src/fockbuild.cpp:64-164).
+//
+// Work decomposition.  Shell pairs (a,b) with l_a >= l_b are grouped into the
+// six angular classes ss, ps, pp, ds, dp, dd and, inside a class, sorted by
+// their Schwarz bound Q_ab (descending).  A unique shell quartet is a pair of
+// pairs {ab, cd}: class(ab) > class(cd), or the same class with index(cd) <=
+// index(ab).  One kernel instantiation per class pair (21 for l <= 2); a block
+// owns one bra pair and a chunk of kets, one thread one quartet.  Because kets
+// are Q-sorted, the kets that can pass Q_ab Q_cd Dmax >= precision form a
+// prefix found by binary search; each quartet then applies molecular2's
+// screen max6(|D| shell blocks) Q_ab Q_cd >= precision (:111-115).
+//
+// Digestion follows :121-153 (6 updates with the permutational degeneracy
+// factor, symmetrised at the end with the 1/4 of :161-162).  J_ab is shared by
+// the whole block and is reduced with warp shuffles before one atomic per
+// element per warp; the other five blocks are accumulated per quartet and
+// added with FP64 atomics.  Everything runs in the Cartesian representation:
+// D is transformed to Cartesian functions first and J, K back afterwards.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "jk_kernels.cuh"
+
+namespace m2 {
+
+static PairView view(const PairClassDev& c) {
+  return PairView{c.sa.p, c.sb.p, c.prim_off.p, c.nprim.p, c.Q.p, c.npair};
+}
+
+static PrimView prim_view(const jk_engine* e) {
+  return PrimView{e->pp_p.p, e->pp_x.p, e->pp_y.p, e->pp_z.p, e->pp_K.p};
+}
+
+static ShellView shell_view(const jk_engine* e) {
+  return ShellView{e->dobs.x.p, e->dobs.y.p, e->dobs.z.p, e->dobs.cart_off.p};
+}
+
+static void launch_schwarz(int la, int lb, const SchwarzParams& P, int npair, cudaStream_t s) {
+  dim3 grid((npair + 63) / 64);
+  if (la == 0 && lb == 0) k_schwarz<0, 0><<<grid, 64, 0, s>>>(P);
+  if (la == 1 && lb == 0) k_schwarz<1, 0><<<grid, 64, 0, s>>>(P);
+  if (la == 1 && lb == 1) k_schwarz<1, 1><<<grid, 64, 0, s>>>(P);
+  if (la == 2 && lb == 0) k_schwarz<2, 0><<<grid, 64, 0, s>>>(P);
+  if (la == 2 && lb == 1) k_schwarz<2, 1><<<grid, 64, 0, s>>>(P);
+  if (la == 2 && lb == 2) launch_schwarz_dd(P, grid, s);
+}
+
+int build_pairs(jk_engine* e) {
+  const HostBasis& hb = e->obs;
+  std::vector<PairClassHost> cls(NPAIRCLASS);
+  for (int la = 0; la <= MAX_L_OBS; ++la)
+    for (int lb = 0; lb <= la; ++lb) {
+      cls[pair_class(la, lb)].la = la;
+      cls[pair_class(la, lb)].lb = lb;
+    }
+  std::vector<double> pp_p, pp_x, pp_y, pp_z, pp_K;
+  for (int i = 0; i < hb.nshell; ++i)
+    for (int j = 0; j < hb.nshell; ++j) {
+      const int li = hb.l[i], lj = hb.l[j];
+      if (li < lj || (li == lj && j > i)) continue;  // canonical orientation l_a >= l_b
+      PairClassHost& c = cls[pair_class(li, lj)];
+      const double* A = &hb.xyz[3 * i];
+      const double* B = &hb.xyz[3 * j];
+      const double AB2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
+      int off = (int)pp_p.size(), cnt = 0;
+      for (int pa = 0; pa < hb.nprim[i]; ++pa)
+        for (int pb = 0; pb < hb.nprim[j]; ++pb) {
+          const double al = hb.exps[hb.prim_off[i] + pa], be = hb.exps[hb.prim_off[j] + pb];
+          const double p = al + be;
+          const double K = hb.coefs[hb.prim_off[i] + pa] * hb.coefs[hb.prim_off[j] + pb] * std::exp(-al * be / p * AB2);
+          if (std::fabs(K) < 1e-18) continue;  // contributes below 1e-18 Eh to any integral
+          pp_p.push_back(p);
+          pp_x.push_back((al * A[0] + be * B[0]) / p);
+          pp_y.push_back((al * A[1] + be * B[1]) / p);
+          pp_z.push_back((al * A[2] + be * B[2]) / p);
+          pp_K.push_back(K);
+          ++cnt;
+        }
+      if (cnt == 0) continue;  // every primitive product vanishes: the pair cannot contribute
+      c.sa.push_back(i);
+      c.sb.push_back(j);
+      c.prim_off.push_back(off);
+      c.nprim.push_back(cnt);
+    }
+  cudaStream_t s = e->stream;
+  cudaError_t st = cudaSuccess;
+  if (st == cudaSuccess) st = e->pp_p.upload(pp_p, s);
+  if (st == cudaSuccess) st = e->pp_x.upload(pp_x, s);
+  if (st == cudaSuccess) st = e->pp_y.upload(pp_y, s);
+  if (st == cudaSuccess) st = e->pp_z.upload(pp_z, s);
+  if (st == cudaSuccess) st = e->pp_K.upload(pp_K, s);
+  if (st != cudaSuccess) return check_cuda(e, st, "upload primitive pairs");
+
+  // Schwarz bounds on the GPU, class by class
+  const int ns = hb.nshell;
+  e->schwarz_host.assign((size_t)ns * ns, 0.0);
+  e->Qmax = 0.0;
+  for (int k = 0; k < NPAIRCLASS; ++k) {
+    PairClassHost& c = cls[k];
+    PairClassDev& d = e->pcls[k];
+    d.la = c.la;
+    d.lb = c.lb;
+    d.npair = (int)c.sa.size();
+    if (d.npair == 0) continue;
+    st = d.sa.upload(c.sa, s);
+    if (st == cudaSuccess) st = d.sb.upload(c.sb, s);
+    if (st == cudaSuccess) st = d.prim_off.upload(c.prim_off, s);
+    if (st == cudaSuccess) st = d.nprim.upload(c.nprim, s);
+    if (st == cudaSuccess) st = d.Q.alloc(d.npair);
+    if (st != cudaSuccess) return check_cuda(e, st, "upload pairs");
+    SchwarzParams P{view(d), prim_view(e), shell_view(e), e->dobs.l.p, e->dobs.pure.p, e->dobs.sph.p,
+                    e->boys.p, d.Q.p};
+    launch_schwarz(c.la, c.lb, P, d.npair, s);
+    c.Q.resize(d.npair);
+    st = cudaMemcpyAsync(c.Q.data(), d.Q.p, d.npair * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (st == cudaSuccess) st = cudaStreamSynchronize(s);
+    if (st != cudaSuccess) return check_cuda(e, st, "schwarz kernel");
+    // sort the class by Q descending
+    std::vector<int> order(d.npair);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return c.Q[x] > c.Q[y]; });
+    PairClassHost sorted;
+    for (int o : order) {
+      sorted.sa.push_back(c.sa[o]);
+      sorted.sb.push_back(c.sb[o]);
+      sorted.prim_off.push_back(c.prim_off[o]);
+      sorted.nprim.push_back(c.nprim[o]);
+      sorted.Q.push_back(c.Q[o]);
+      e->schwarz_host[(size_t)c.sa[o] * ns + c.sb[o]] = c.Q[o];
+      e->schwarz_host[(size_t)c.sb[o] * ns + c.sa[o]] = c.Q[o];
+      e->Qmax = std::max(e->Qmax, c.Q[o]);
+    }
+    st = d.sa.upload(sorted.sa, s);
+    if (st == cudaSuccess) st = d.sb.upload(sorted.sb, s);
+    if (st == cudaSuccess) st = d.prim_off.upload(sorted.prim_off, s);
+    if (st == cudaSuccess) st = d.nprim.upload(sorted.nprim, s);
+    if (st == cudaSuccess) st = d.Q.upload(sorted.Q, s);
+    if (st == cudaSuccess) st = cudaStreamSynchronize(s);
+    if (st != cudaSuccess) return check_cuda(e, st, "upload sorted pairs");
+  }
+  st = e->schwarz_dev.upload(e->schwarz_host, s);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(s);
+  return check_cuda(e, st, "schwarz matrix");
+}
+
+static void launch_jk(int A, int B, const JKParams& P, int nbra, int nket_max, cudaStream_t s) {
+  dim3 grid(nbra, (nket_max + P.kchunk - 1) / P.kchunk);
+  if (A <= 2)
+    launch_jk_bra_s(A, B, P, grid, s);
+  else if (A == 3)
+    launch_jk_bra_ds(B, P, grid, s);
+  else if (A == 4)
+    launch_jk_bra_dp(B, P, grid, s);
+  else if (B < 4)
+    launch_jk_bra_dd_lo(B, P, grid, s);
+  else
+    launch_jk_bra_dd_hi(B, P, grid, s);
+}
+
+int direct_jk_device(jk_engine* e, const double* dD, double precision, double mult, double* dJ, double* dK,
+                     cudaStream_t s) {
+  const int nc = e->obs.n_cart, ns = e->obs.nshell;
+  cudaError_t st = cudaSuccess;
+  if (st == cudaSuccess) st = e->Dcart.alloc((size_t)nc * nc);
+  if (st == cudaSuccess) st = e->Jcart.alloc((size_t)nc * nc);
+  if (st == cudaSuccess) st = e->Kcart.alloc((size_t)nc * nc);
+  if (st == cudaSuccess) st = e->Dnorm.alloc((size_t)ns * ns);
+  if (st == cudaSuccess) st = e->Dmax.alloc(2);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_direct scratch");
+  launch_shell_norms(e, dD, e->Dnorm.p, e->Dmax.p, s);
+  launch_final_to_cart(e, dD, e->Dcart.p, s);
+  cudaMemsetAsync(e->Jcart.p, 0, sizeof(double) * nc * nc, s);
+  cudaMemsetAsync(e->Kcart.p, 0, sizeof(double) * nc * nc, s);
+  unsigned long long* counter = reinterpret_cast<unsigned long long*>(e->Dmax.p + 1);
+  cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+  JKParams P{};
+  P.pp = prim_view(e);
+  P.sh = shell_view(e);
+  P.Dnorm = e->Dnorm.p;
+  P.nshell = ns;
+  P.Dmax = e->Dmax.p;
+  P.Dc = e->Dcart.p;
+  P.nc = nc;
+  P.Jc = e->Jcart.p;
+  P.Kc = e->Kcart.p;
+  P.precision = precision;
+  P.boys = e->boys.p;
+  P.counter = counter;
+  P.kchunk = 512;
+  for (int A = 0; A < NPAIRCLASS; ++A)
+    for (int B = 0; B <= A; ++B) {
+      const PairClassDev& bra = e->pcls[A];
+      const PairClassDev& ket = e->pcls[B];
+      if (bra.npair == 0 || ket.npair == 0) continue;
+      P.bra = view(bra);
+      P.ket = view(ket);
+      P.same_class = (A == B);
+      launch_jk(A, B, P, bra.npair, ket.npair, s);
+    }
+  // J = 1/4 (J + J^T) mult, K = 1/2 * 1/4 (K + K^T) mult  (src/fockbuild.cpp:146-149, 161-162)
+  launch_cart_to_final_sym(e, e->Jcart.p, 0.25 * mult, dJ, s);
+  launch_cart_to_final_sym(e, e->Kcart.p, 0.125 * mult, dK, s);
+  return check_cuda(e, cudaGetLastError(), "jk_direct launch");
+}
+
+}  // namespace m2
+
+using namespace m2;
+
+extern "C" {
+
+int jk_direct_device(jk_engine* e, const double* dD, double precision, double multiplier, double* dJ, double* dK,
+                     void* stream) {
+  if (!e || !dD || !dJ || !dK) return JK_ERR_ARG;
+  if (!(precision >= 0.0)) return set_error(e, JK_ERR_ARG, "jk_direct: precision must be >= 0");
+  cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+  return direct_jk_device(e, dD, precision, multiplier, dJ, dK, s);
+}
+
+int jk_direct(jk_engine* e, const double* D, double precision, double multiplier, double* J, double* K) {
+  if (!e || !D || !J || !K) return JK_ERR_ARG;
+  const int n = e->obs.n_final;
+  const size_t bytes = sizeof(double) * n * n;
+  cudaError_t st = cudaSuccess;
+  if (st == cudaSuccess) st = e->Dfinal.alloc((size_t)n * n);
+  if (st == cudaSuccess) st = e->Jfinal.alloc((size_t)n * n);
+  if (st == cudaSuccess) st = e->Kfinal.alloc((size_t)n * n);
+  if (st == cudaSuccess) st = cudaMemcpyAsync(e->Dfinal.p, D, bytes, cudaMemcpyHostToDevice, e->stream);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_direct upload");
+  int rc = jk_direct_device(e, e->Dfinal.p, precision, multiplier, e->Jfinal.p, e->Kfinal.p, nullptr);
+  if (rc) return rc;
+  st = cudaMemcpyAsync(J, e->Jfinal.p, bytes, cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaMemcpyAsync(K, e->Kfinal.p, bytes, cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
+  return check_cuda(e, st, "jk_direct download");
+}
+
+}  // extern "C"

@@ -1,0 +1,158 @@
+"""ctypes binding of ``libm2jk.so`` shaped like molecular2's ``IntegralEngine`` / ``Fock``.
+
+The product path is the CUDA library; there is no CPU fallback.  Importing
+works without a GPU, but creating an engine needs the built library and a
+CUDA device and raises otherwise.
+
+Reference surface mirrored here (molecular2 paths):
+  * ``IntegralEngine.getPrescreen`` / ``compute_schwarz_ints`` (src/integrals.cpp:95, 472-513)
+  * ``Fock.formJKdirect(Schwarz, D, multiplier)``   (src/fockbuild.cpp:64-164)
+  * ``Fock.getJ / getK / getJK``                     (inc/fock.hpp:141-143)
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .basis import BasisSet
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libm2jk.so")
+
+JK_ERRORS = {1: "JK_ERR_ARG", 2: "JK_ERR_CUDA", 3: "JK_ERR_NOT_PD", 4: "JK_ERR_STATE", 5: "JK_ERR_NOMEM",
+             6: "JK_ERR_NOT_CONVERGED"}
+
+_lib = None
+
+# exported symbols and their C signatures (restype, argtypes)
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+SIGNATURES = {
+    "jk_create": (_I, [_P, _P, _I, _P, _P, _I, ctypes.POINTER(_P)]),
+    "jk_destroy": (None, [_P]),
+    "jk_last_error": (ctypes.c_char_p, [_P]),
+    "jk_sizes": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "jk_schwarz": (_I, [_P, _P]),
+    "jk_direct": (_I, [_P, _P, _D, _D, _P, _P]),
+    "jk_direct_device": (_I, [_P, _P, _D, _D, _P, _P, _P]),
+    "jk_last_quartets": (ctypes.c_longlong, [_P]),
+}
+
+
+class JKError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{JK_ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load_library(path=LIBPATH):
+    """Load the engine; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is missing: run `python -m molecular2_b200.build` first")
+        L = ctypes.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _bp(basis):
+    return ctypes.cast(ctypes.pointer(basis.struct()), ctypes.c_void_p)
+
+
+class IntegralEngine:
+    """Owns one ``jk_engine``: the device basis, shell pairs, Schwarz bounds and scratch."""
+
+    def __init__(self, obs: BasisSet, aux: BasisSet = None, device=0):
+        self.lib = load_library()
+        self.obs = obs
+        self.aux = aux
+        mol = obs.mol
+        self._Z = np.ascontiguousarray(mol.Z, dtype=np.float64)
+        self._xyz = np.ascontiguousarray(mol.xyz.reshape(-1), dtype=np.float64)
+        h = ctypes.c_void_p()
+        rc = self.lib.jk_create(_bp(obs), _bp(aux) if aux is not None else None, mol.natom, _p(self._xyz),
+                                _p(self._Z), device, ctypes.byref(h))
+        self.h = h
+        if rc:
+            msg = self.lib.jk_last_error(h).decode() if h else "allocation failed"
+            self.close()
+            raise JKError(rc, msg)
+        n, na, ns = _I(), _I(), _I()
+        self.lib.jk_sizes(self.h, ctypes.byref(n), ctypes.byref(na), ctypes.byref(ns))
+        self.n, self.naux, self.nshell = n.value, na.value, ns.value
+
+    def _check(self, rc):
+        if rc:
+            raise JKError(rc, self.lib.jk_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.jk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def getPrescreen(self):
+        Q = np.zeros((self.nshell, self.nshell))
+        self._check(self.lib.jk_schwarz(self.h, _p(Q)))
+        return Q
+
+    compute_schwarz_ints = getPrescreen
+
+    def last_quartets(self):
+        return int(self.lib.jk_last_quartets(self.h))
+
+    # -- direct J/K ----------------------------------------------------------
+    def jk_direct(self, D, precision=1e-12, multiplier=1.0):
+        n = self.n
+        D = np.asfortranarray(D, dtype=np.float64)
+        J = np.zeros((n, n), order="F")
+        K = np.zeros((n, n), order="F")
+        self._check(self.lib.jk_direct(self.h, _p(D), precision, multiplier, _p(J), _p(K)))
+        return J, K
+
+    def jk_direct_device(self, dD, dJ, dK, precision=1e-12, multiplier=1.0, stream=None):
+        """Device-pointer variant (ints from e.g. torch ``data_ptr()``)."""
+        self._check(self.lib.jk_direct_device(self.h, ctypes.c_void_p(dD), precision, multiplier,
+                                              ctypes.c_void_p(dJ), ctypes.c_void_p(dK),
+                                              ctypes.c_void_p(stream) if stream else None))
+
+
+class Fock:
+    """The J/K part of molecular2's ``Fock`` on the GPU engine."""
+
+    def __init__(self, engine: IntegralEngine, precision=1e-12):
+        self.integrals = engine
+        self.precision = precision
+        self.jints = self.kints = self.jkints = None
+
+    def formJKdirect(self, Schwarz, D, multiplier=1.0):
+        """src/fockbuild.cpp:64-164 — the Schwarz argument is the engine's own
+        (computed on the device at creation); passing None keeps it."""
+        J, K = self.integrals.jk_direct(D, self.precision, multiplier)
+        self.jints, self.kints = J, K
+        self.jkints = J - 0.5 * K
+        return self.jkints
+
+    def getJ(self):
+        return self.jints
+
+    def getK(self):
+        return self.kints
+
+    def getJK(self):
+        return self.jkints
