@@ -85,6 +85,66 @@ int jk_direct_device(jk_engine* e, const double* dD, double precision, double mu
 /* Number of shell quartets the last direct build evaluated. */
 long long jk_last_quartets(const jk_engine* e);
 
+/* Three-index integrals (P|mn) in molecular2's packed layout: column-major
+ * (n(n+1)/2) x naux, row x(x+1)/2 + y for x >= y.
+ * Replaces IntegralEngine::compute_eris_3index(obs, auxbs, Matrix&)
+ * (src/eris.cpp:89-156). */
+int jk_eri3(jk_engine* e, double* T);
+
+/* Two-index metric (P|Q), naux x naux.
+ * Replaces IntegralEngine::compute_eris_2index (src/eris.cpp:304-356). */
+int jk_eri2(jk_engine* e, double* V);
+
+/* First-call part of compute_2body_fock_df (src/fockbuild.cpp:598-619):
+ * (P|mn), (P|Q), the Cholesky factor V = L L^T and B = (mn|P) L^-T, kept in
+ * HBM.  Returns JK_ERR_NOT_PD when the metric is not positive definite. */
+int jk_df_setup(jk_engine* e);
+
+/* Per-iteration part of compute_2body_fock_df (src/fockbuild.cpp:621-659):
+ * J and K with respect to Cocc Cocc^T (the caller forms mult*(2J - K) as
+ * Fock::formJKdf does at :173).  prec_mode 0 = FP64.  Host pointers. */
+int jk_df(jk_engine* e, const double* Cocc, int nocc, int prec_mode, double* J, double* K);
+int jk_df_device(jk_engine* e, const double* dCocc, int nocc, int prec_mode, double* dJ, double* dK, void* stream);
+
+/* Overlap, kinetic and nuclear-attraction matrices (point charges of
+ * jk_create): IntegralEngine::compute_1body_ints (src/integrals.cpp:394-449). */
+int jk_one_body(jk_engine* e, double* S, double* T, double* V);
+
+/* RHF SCF with every n x n matrix in HBM: SCF::rhf (src/scf.cpp:90-185) with
+ * DIISEngine (src/diis.cpp:22-116), the incremental direct Fock build of
+ * Fock::makeFock (src/fockbuild.cpp:176-222) and Fock::formJKdf for df != 0.
+ * Converged when ||D - D_old||_F < densconverge and |dE| < enconverge (:156).
+ * Returns JK_ERR_NOT_CONVERGED (result still filled) after maxiter. */
+typedef struct jk_scf_options {
+  int nocc;
+  int df;                  /* 0 = integral-direct J/K, 1 = density-fitted */
+  int prec_mode;           /* DF only: 0 = FP64 */
+  int maxiter;             /* molecular2 default 40 */
+  int maxdiis;             /* default 8 */
+  int diis;                /* 1 = on */
+  double precision;        /* Schwarz x density screening threshold, default 1e-12 */
+  double enconverge;       /* default 1e-7 */
+  double densconverge;     /* default 1e-4 */
+  double enuc;             /* nuclear repulsion energy added to E */
+  const double* guess_fock;  /* host n x n AO Fock for the first diagonalisation, NULL = core Hamiltonian */
+  double* out_density;     /* optional host n x n */
+  double* out_coeffs;      /* optional host n x n (MO coefficients, columns) */
+  double* out_eps;         /* optional host n */
+} jk_scf_options;
+
+typedef struct jk_scf_result {
+  double energy;
+  int iterations;
+  int converged;
+  int jk_builds;
+  double jk_ms;            /* device time inside J/K builds */
+  double total_ms;         /* host wall time of the whole call */
+  double last_delta_e;
+  double last_delta_d;
+} jk_scf_result;
+
+int jk_scf_rhf(jk_engine* e, const jk_scf_options* opt, jk_scf_result* res);
+
 #ifdef __cplusplus
 }
 #endif

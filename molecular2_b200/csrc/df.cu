@@ -1,0 +1,391 @@
+// Density-fitted J/K (Fock::formJKdf / compute_2body_fock_df, molecular2
+// src/fockbuild.cpp:171-174, 585-660), the three- and two-index integrals
+// (IntegralEngine::compute_eris_3index/2index, src/eris.cpp:89-156, 304-356)
+// and the one-body S, T, V matrices (IntegralEngine constructor,
+// src/integrals.cpp:70-72).
+//
+// HBM layout.  The fitted three-index tensor is stored unpacked as
+// B[x][K][y] (n x naux x n, x slowest): for every orbital x the slab B[x] is
+// naux x n with y contiguous.  With that layout
+//   X[x][K][i] = sum_y B[x][K][y] C[y][i]    is one GEMM (n*naux x n) . (n x o),
+//   K          = X X^T                        is one SYRK over the n x (naux*o) matrix X,
+//   gamma_K    = sum_{x,i} X[x][K][i] C[x][i] and
+//   J[x][y]    = sum_K gamma_K B[x][K][y]     stream X and B once each.
+// B = T L^-T with V = L L^T is formed once per geometry by a strided-batched
+// GEMM with L^-1 (the reference's O(n^2 naux^2) transform at :610-618).
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "df_kernels.cuh"
+#include "engine.h"
+
+namespace m2 {
+
+PrimView prim_view(const jk_engine* e);
+ShellView shell_view(const jk_engine* e);
+
+static int prepare_aux(jk_engine* e) {
+  if (!e->has_aux) return set_error(e, JK_ERR_STATE, "no fitting basis was given to jk_create");
+  if (e->ap_p.p) return JK_OK;
+  const HostBasis& a = e->aux;
+  std::vector<double> p, x, y, z, K;
+  std::vector<int> off;
+  for (int s = 0; s < a.nshell; ++s) {
+    off.push_back((int)p.size());
+    for (int k = 0; k < a.nprim[s]; ++k) {
+      p.push_back(a.exps[a.prim_off[s] + k]);
+      x.push_back(a.xyz[3 * s]);
+      y.push_back(a.xyz[3 * s + 1]);
+      z.push_back(a.xyz[3 * s + 2]);
+      K.push_back(a.coefs[a.prim_off[s] + k]);
+    }
+  }
+  cudaStream_t st = e->stream;
+  cudaError_t r = e->ap_p.upload(p, st);
+  if (r == cudaSuccess) r = e->ap_x.upload(x, st);
+  if (r == cudaSuccess) r = e->ap_y.upload(y, st);
+  if (r == cudaSuccess) r = e->ap_z.upload(z, st);
+  if (r == cudaSuccess) r = e->ap_K.upload(K, st);
+  if (r == cudaSuccess) r = e->aux_prim_off.upload(off, st);
+  for (int l = 0; l <= MAX_L_AUX && r == cudaSuccess; ++l) {
+    std::vector<int> sh;
+    for (int s = 0; s < a.nshell; ++s)
+      if (a.l[s] == l) sh.push_back(s);
+    e->aux_by_l_count[l] = (int)sh.size();
+    r = e->aux_by_l[l].upload(sh, st);
+  }
+  if (r == cudaSuccess) r = cudaStreamSynchronize(st);
+  return check_cuda(e, r, "prepare fitting basis");
+}
+
+static PrimView aux_view(const jk_engine* e) {
+  return PrimView{e->ap_p.p, e->ap_x.p, e->ap_y.p, e->ap_z.p, e->ap_K.p};
+}
+
+// T3[x][P][y] = (P|xy), full n x naux x n.
+static int compute_T3(jk_engine* e, double* T3, cudaStream_t s) {
+  const int n = e->obs.n_final, naux = e->aux.n_final;
+  cudaMemsetAsync(T3, 0, sizeof(double) * (size_t)n * naux * n, s);
+  for (int l = 0; l <= MAX_L_AUX; ++l) {
+    if (!e->aux_by_l_count[l]) continue;
+    for (int pc = 0; pc < NPAIRCLASS; ++pc) {
+      if (!e->pcls[pc].npair) continue;
+      Eri3Params P{};
+      P.ap = aux_view(e);
+      P.aux_shells = e->aux_by_l[l].p;
+      P.naux_shells = e->aux_by_l_count[l];
+      P.aux_prim_off = e->aux_prim_off.p;
+      P.aux_nprim = e->daux.nprim.p;
+      P.ax = e->daux.x.p;
+      P.ay = e->daux.y.p;
+      P.az = e->daux.z.p;
+      P.aux_foff = e->daux.final_off.p;
+      P.aux_pure = e->daux.pure.p;
+      P.pairs = view(e->pcls[pc]);
+      P.pp = prim_view(e);
+      P.ox = e->dobs.x.p;
+      P.oy = e->dobs.y.p;
+      P.oz = e->dobs.z.p;
+      P.obs_foff = e->dobs.final_off.p;
+      P.obs_pure = e->dobs.pure.p;
+      P.sph = e->dobs.sph.p;
+      P.boys = e->boys.p;
+      P.n = n;
+      P.naux = naux;
+      P.T3 = T3;
+      if (l == 0) launch_eri3_l0(pc, P, s);
+      if (l == 1) launch_eri3_l1(pc, P, s);
+      if (l == 2) launch_eri3_l2(pc, P, s);
+      if (l == 3) launch_eri3_l3(pc, P, s);
+    }
+  }
+  return check_cuda(e, cudaGetLastError(), "eri3 launch");
+}
+
+static int compute_V(jk_engine* e, double* V, cudaStream_t s) {
+  const int naux = e->aux.n_final;
+  for (int lp = 0; lp <= MAX_L_AUX; ++lp)
+    for (int lq = 0; lq <= lp; ++lq) {
+      if (!e->aux_by_l_count[lp] || !e->aux_by_l_count[lq]) continue;
+      Eri2Params P{};
+      P.ap = aux_view(e);
+      P.shells_p = e->aux_by_l[lp].p;
+      P.np = e->aux_by_l_count[lp];
+      P.shells_q = e->aux_by_l[lq].p;
+      P.nq = e->aux_by_l_count[lq];
+      P.aux_prim_off = e->aux_prim_off.p;
+      P.aux_nprim = e->daux.nprim.p;
+      P.ax = e->daux.x.p;
+      P.ay = e->daux.y.p;
+      P.az = e->daux.z.p;
+      P.aux_foff = e->daux.final_off.p;
+      P.aux_pure = e->daux.pure.p;
+      P.sph = e->dobs.sph.p;
+      P.boys = e->boys.p;
+      P.naux = naux;
+      P.V = V;
+      launch_eri2(lp, lq, P, s);
+    }
+  return check_cuda(e, cudaGetLastError(), "eri2 launch");
+}
+
+// packed reference layout: Tp[(x(x+1)/2 + y) + P*npair], x >= y
+__global__ void k_pack_T3(int n, int naux, const double* __restrict__ T3, double* __restrict__ Tp) {
+  const size_t npair = (size_t)n * (n + 1) / 2;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= npair * naux) return;
+  const int P = (int)(idx / npair);
+  const size_t xy = idx % npair;
+  int x = (int)floor((sqrt(8.0 * (double)xy + 1.0) - 1.0) * 0.5);
+  while ((size_t)x * (x + 1) / 2 > xy) --x;
+  while ((size_t)(x + 1) * (x + 2) / 2 <= xy) ++x;
+  const int y = (int)(xy - (size_t)x * (x + 1) / 2);
+  Tp[idx] = T3[((size_t)x * naux + P) * n + y];
+}
+
+__global__ void k_identity(int n, double* A) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < (size_t)n * n) A[i] = (i % (n + 1) == 0) ? 1.0 : 0.0;
+}
+
+__global__ void k_lower_only(int n, double* A) {  // zero the strict upper triangle (col-major)
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < (size_t)n * n && (int)(i % n) < (int)(i / n)) A[i] = 0.0;
+}
+
+__global__ void k_sym_from_lower(int n, double* A) {  // A[j][i] = A[i][j] for i > j (col-major lower)
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (size_t)n * n) return;
+  const int r = (int)(k % n), c = (int)(k / n);
+  if (r < c) A[k] = A[(size_t)r * n + c];
+}
+
+// gamma_K = sum_{x,i} X[x][K][i] C[x][i]   (C column-major n x o)
+__global__ void k_gamma(int n, int naux, int o, const double* __restrict__ X, const double* __restrict__ C,
+                        double* __restrict__ g) {
+  const int K = blockIdx.x;
+  double acc = 0.0;
+  for (int idx = threadIdx.x; idx < n * o; idx += blockDim.x) {
+    const int x = idx / o, i = idx % o;
+    acc += X[((size_t)x * naux + K) * o + i] * C[(size_t)i * n + x];
+  }
+  __shared__ double red[32];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    acc = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (threadIdx.x == 0) g[K] = acc;
+  }
+}
+
+// J[x][y] = sum_K gamma_K B[x][K][y]; one block per x, threads over y.
+__global__ void k_df_J(int n, int naux, const double* __restrict__ B, const double* __restrict__ g,
+                       double* __restrict__ J) {
+  const int x = blockIdx.x;
+  for (int y = threadIdx.x; y < n; y += blockDim.x) {
+    double acc = 0.0;
+    const double* b = B + (size_t)x * naux * n + y;
+    for (int K = 0; K < naux; ++K) acc += __ldg(g + K) * b[(size_t)K * n];
+    J[(size_t)y * n + x] = acc;
+  }
+}
+
+int df_setup(jk_engine* e) {
+  int rc = prepare_aux(e);
+  if (rc) return rc;
+  cudaStream_t s = e->stream;
+  const int n = e->obs.n_final, naux = e->aux.n_final;
+  DFState& d = e->df;
+  DevBuf<double> T3, Linv;
+  cudaError_t st = T3.alloc((size_t)n * naux * n);
+  if (st == cudaSuccess) st = d.L.alloc((size_t)naux * naux);
+  if (st == cudaSuccess) st = Linv.alloc((size_t)naux * naux);
+  if (st == cudaSuccess) st = d.B64.alloc((size_t)n * naux * n);
+  if (st != cudaSuccess) return check_cuda(e, st, "df_setup allocation");
+  if ((rc = compute_T3(e, T3.p, s))) return rc;
+  if ((rc = compute_V(e, d.L.p, s))) return rc;
+  // V = L L^T (cuSOLVER potrf, lower)
+  int lwork = 0;
+  if (cusolverDnDpotrf_bufferSize(e->cusolver, CUBLAS_FILL_MODE_LOWER, naux, d.L.p, naux, &lwork) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return set_error(e, JK_ERR_CUDA, "potrf buffer size");
+  DevBuf<double> work;
+  DevBuf<int> info;
+  st = work.alloc(lwork > 0 ? lwork : 1);
+  if (st == cudaSuccess) st = info.alloc(1);
+  if (st != cudaSuccess) return check_cuda(e, st, "potrf workspace");
+  if (cusolverDnDpotrf(e->cusolver, CUBLAS_FILL_MODE_LOWER, naux, d.L.p, naux, work.p, lwork, info.p) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return set_error(e, JK_ERR_CUDA, "potrf");
+  int hinfo = 0;
+  st = cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(s);
+  if (st != cudaSuccess) return check_cuda(e, st, "potrf");
+  if (hinfo != 0)
+    return set_error(e, JK_ERR_NOT_PD,
+                     "fitting metric (P|Q) is not positive definite (leading minor " + std::to_string(hinfo) + ")");
+  const int nb = 256;
+  k_lower_only<<<(unsigned)(((size_t)naux * naux + nb - 1) / nb), nb, 0, s>>>(naux, d.L.p);
+  k_identity<<<(unsigned)(((size_t)naux * naux + nb - 1) / nb), nb, 0, s>>>(naux, Linv.p);
+  const double one = 1.0, zero = 0.0;
+  cublasSetStream(e->cublas, s);
+  if (cublasDtrsm(e->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, naux,
+                  naux, &one, d.L.p, naux, Linv.p, naux) != CUBLAS_STATUS_SUCCESS)
+    return set_error(e, JK_ERR_CUDA, "trsm for L^-1");
+  // B[x]^T (n x naux, ld n) = T[x]^T (n x naux) . Linv^T
+  if (cublasDgemmStridedBatched(e->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n, naux, naux, &one, T3.p, n,
+                                (long long)naux * n, Linv.p, naux, 0, &zero, d.B64.p, n, (long long)naux * n,
+                                n) != CUBLAS_STATUS_SUCCESS)
+    return set_error(e, JK_ERR_CUDA, "B = T L^-T gemm");
+  st = cudaStreamSynchronize(s);
+  if (st != cudaSuccess) return check_cuda(e, st, "df_setup");
+  d.naux = naux;
+  d.ready = true;
+  return JK_OK;
+}
+
+int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ, double* dK, cudaStream_t s) {
+  DFState& d = e->df;
+  if (!d.ready) return set_error(e, JK_ERR_STATE, "jk_df before jk_df_setup");
+  if (mode != 0) return set_error(e, JK_ERR_ARG, "jk_df: unsupported precision mode");
+  const int n = e->obs.n_final, naux = d.naux;
+  cudaError_t st = d.X64.alloc((size_t)n * naux * nocc);
+  if (st == cudaSuccess) st = d.gamma.alloc(naux);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_df scratch");
+  const double one = 1.0, zero = 0.0;
+  cublasSetStream(e->cublas, s);
+  // X (o x n*naux, col-major) = C^T . B   ->  X[x][K][i]
+  if (cublasDgemm(e->cublas, CUBLAS_OP_T, CUBLAS_OP_N, nocc, n * naux, n, &one, dC, n, d.B64.p, n, &zero, d.X64.p,
+                  nocc) != CUBLAS_STATUS_SUCCESS)
+    return set_error(e, JK_ERR_CUDA, "X = B C gemm");
+  // K = X^T X over the (naux*o) inner index
+  if (cublasDsyrk(e->cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, naux * nocc, &one, d.X64.p, naux * nocc, &zero,
+                  dK, n) != CUBLAS_STATUS_SUCCESS)
+    return set_error(e, JK_ERR_CUDA, "K = X X^T syrk");
+  const int nb = 256;
+  k_sym_from_lower<<<(unsigned)(((size_t)n * n + nb - 1) / nb), nb, 0, s>>>(n, dK);
+  k_gamma<<<naux, 256, 0, s>>>(n, naux, nocc, d.X64.p, dC, d.gamma.p);
+  k_df_J<<<n, 128, 0, s>>>(n, naux, d.B64.p, d.gamma.p, dJ);
+  return check_cuda(e, cudaGetLastError(), "jk_df launch");
+}
+
+int one_body_device(jk_engine* e, double* S, double* T, double* V, cudaStream_t s) {
+  const int n = e->obs.n_final;
+  DevBuf<double> Z, C;
+  cudaError_t st = Z.upload(e->Z, s);
+  if (st == cudaSuccess) st = C.upload(e->atom_xyz, s);
+  if (st != cudaSuccess) return check_cuda(e, st, "one_body upload");
+  for (int pc = 0; pc < NPAIRCLASS; ++pc) {
+    if (!e->pcls[pc].npair) continue;
+    OneBodyParams P{};
+    P.pairs = view(e->pcls[pc]);
+    P.pp = prim_view(e);
+    P.pa = e->pp_a.p;
+    P.ox = e->dobs.x.p;
+    P.oy = e->dobs.y.p;
+    P.oz = e->dobs.z.p;
+    P.foff = e->dobs.final_off.p;
+    P.pure = e->dobs.pure.p;
+    P.sph = e->dobs.sph.p;
+    P.boys = e->boys.p;
+    P.natom = e->natom;
+    P.Z = Z.p;
+    P.cxyz = C.p;
+    P.n = n;
+    P.S = S;
+    P.T = T;
+    P.V = V;
+    launch_onebody(pc, P, s);
+  }
+  st = cudaGetLastError();
+  if (st == cudaSuccess) st = cudaStreamSynchronize(s);  // Z, C die on return
+  return check_cuda(e, st, "one_body");
+}
+
+}  // namespace m2
+
+using namespace m2;
+
+extern "C" {
+
+int jk_eri3(jk_engine* e, double* Tpacked) {
+  if (!e || !Tpacked) return JK_ERR_ARG;
+  int rc = prepare_aux(e);
+  if (rc) return rc;
+  const int n = e->obs.n_final, naux = e->aux.n_final;
+  const size_t npair = (size_t)n * (n + 1) / 2;
+  DevBuf<double> T3, Tp;
+  cudaError_t st = T3.alloc((size_t)n * naux * n);
+  if (st == cudaSuccess) st = Tp.alloc(npair * naux);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_eri3 allocation");
+  if ((rc = compute_T3(e, T3.p, e->stream))) return rc;
+  const size_t tot = npair * naux;
+  k_pack_T3<<<(unsigned)((tot + 255) / 256), 256, 0, e->stream>>>(n, naux, T3.p, Tp.p);
+  st = cudaMemcpyAsync(Tpacked, Tp.p, tot * sizeof(double), cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
+  return check_cuda(e, st, "jk_eri3");
+}
+
+int jk_eri2(jk_engine* e, double* V) {
+  if (!e || !V) return JK_ERR_ARG;
+  int rc = prepare_aux(e);
+  if (rc) return rc;
+  const int naux = e->aux.n_final;
+  DevBuf<double> Vd;
+  cudaError_t st = Vd.alloc((size_t)naux * naux);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_eri2 allocation");
+  if ((rc = compute_V(e, Vd.p, e->stream))) return rc;
+  st = cudaMemcpyAsync(V, Vd.p, sizeof(double) * naux * naux, cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
+  return check_cuda(e, st, "jk_eri2");
+}
+
+int jk_df_setup(jk_engine* e) {
+  if (!e) return JK_ERR_ARG;
+  return df_setup(e);
+}
+
+int jk_df_device(jk_engine* e, const double* dC, int nocc, int prec_mode, double* dJ, double* dK, void* stream) {
+  if (!e || !dC || !dJ || !dK || nocc <= 0) return JK_ERR_ARG;
+  return df_jk_device(e, dC, nocc, prec_mode, dJ, dK, stream ? (cudaStream_t)stream : e->stream);
+}
+
+int jk_df(jk_engine* e, const double* C, int nocc, int prec_mode, double* J, double* K) {
+  if (!e || !C || !J || !K || nocc <= 0) return JK_ERR_ARG;
+  const int n = e->obs.n_final;
+  DevBuf<double> dC;
+  cudaError_t st = dC.alloc((size_t)n * nocc);
+  if (st == cudaSuccess) st = e->Jfinal.alloc((size_t)n * n);
+  if (st == cudaSuccess) st = e->Kfinal.alloc((size_t)n * n);
+  if (st == cudaSuccess) st = cudaMemcpyAsync(dC.p, C, sizeof(double) * n * nocc, cudaMemcpyHostToDevice, e->stream);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_df upload");
+  int rc = df_jk_device(e, dC.p, nocc, prec_mode, e->Jfinal.p, e->Kfinal.p, e->stream);
+  if (rc) return rc;
+  st = cudaMemcpyAsync(J, e->Jfinal.p, sizeof(double) * n * n, cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaMemcpyAsync(K, e->Kfinal.p, sizeof(double) * n * n, cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
+  return check_cuda(e, st, "jk_df download");
+}
+
+int jk_one_body(jk_engine* e, double* S, double* T, double* V) {
+  if (!e || !S || !T || !V) return JK_ERR_ARG;
+  const int n = e->obs.n_final;
+  DevBuf<double> dS, dT, dV;
+  cudaError_t st = dS.alloc((size_t)n * n);
+  if (st == cudaSuccess) st = dT.alloc((size_t)n * n);
+  if (st == cudaSuccess) st = dV.alloc((size_t)n * n);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_one_body allocation");
+  int rc = one_body_device(e, dS.p, dT.p, dV.p, e->stream);
+  if (rc) return rc;
+  const size_t b = sizeof(double) * n * n;
+  st = cudaMemcpyAsync(S, dS.p, b, cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaMemcpyAsync(T, dT.p, b, cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaMemcpyAsync(V, dV.p, b, cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
+  return check_cuda(e, st, "jk_one_body");
+}
+
+}  // extern "C"

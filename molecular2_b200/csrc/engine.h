@@ -78,10 +78,11 @@ struct PairClassDev {
 
 struct DFState {
   bool ready = false;
-  int naux = 0, npair_bf = 0;
+  int naux = 0;
   DevBuf<double> B64;      // [x][K][y] unpacked, FP64
-  DevBuf<float> B32;       // same layout, FP32 copy for the mixed path
   DevBuf<double> L;        // Cholesky factor of the metric (naux x naux, col-major)
+  DevBuf<double> X64;      // [x][K][i]
+  DevBuf<double> gamma;    // naux
 };
 
 }  // namespace m2
@@ -102,7 +103,11 @@ struct jk_engine {
 
   // shell pairs (orbital basis)
   m2::PairClassDev pcls[m2::NPAIRCLASS];
-  m2::DevBuf<double> pp_p, pp_x, pp_y, pp_z, pp_K;  // primitive pairs
+  m2::DevBuf<double> pp_p, pp_x, pp_y, pp_z, pp_K, pp_a;  // primitive pairs (pp_a: exponent of shell a)
+  m2::DevBuf<double> ap_p, ap_x, ap_y, ap_z, ap_K;         // fitting primitives as (P, unit) pairs
+  m2::DevBuf<int> aux_prim_off;                           // per fitting shell
+  m2::DevBuf<int> aux_by_l[m2::MAX_L_AUX + 1];             // fitting shells grouped by l
+  int aux_by_l_count[m2::MAX_L_AUX + 1] = {0, 0, 0, 0};
   std::vector<double> schwarz_host;                  // nshell x nshell, row-major (symmetric)
   m2::DevBuf<double> schwarz_dev;                    // nshell x nshell
   double Qmax = 0.0;
@@ -125,6 +130,10 @@ int upload_basis(jk_engine* e, const HostBasis& hb, DevBasis& db);
 int build_pairs(jk_engine* e);
 int direct_jk_device(jk_engine* e, const double* dD, double precision, double mult, double* dJ, double* dK,
                      cudaStream_t s);
+// df.cu
+int df_setup(jk_engine* e);
+int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ, double* dK, cudaStream_t s);
+int one_body_device(jk_engine* e, double* S, double* T, double* V, cudaStream_t s);
 // transforms (cart <-> final) and norms
 void launch_final_to_cart(const jk_engine* e, const double* Dfinal, double* Dcart, cudaStream_t s);
 void launch_cart_to_final_sym(const jk_engine* e, const double* Xcart, double scale, double* Xfinal, cudaStream_t s);

@@ -28,15 +28,11 @@
 
 namespace m2 {
 
-static PairView view(const PairClassDev& c) {
-  return PairView{c.sa.p, c.sb.p, c.prim_off.p, c.nprim.p, c.Q.p, c.npair};
-}
+PairView view(const PairClassDev& c) { return PairView{c.sa.p, c.sb.p, c.prim_off.p, c.nprim.p, c.Q.p, c.npair}; }
 
-static PrimView prim_view(const jk_engine* e) {
-  return PrimView{e->pp_p.p, e->pp_x.p, e->pp_y.p, e->pp_z.p, e->pp_K.p};
-}
+PrimView prim_view(const jk_engine* e) { return PrimView{e->pp_p.p, e->pp_x.p, e->pp_y.p, e->pp_z.p, e->pp_K.p}; }
 
-static ShellView shell_view(const jk_engine* e) {
+ShellView shell_view(const jk_engine* e) {
   return ShellView{e->dobs.x.p, e->dobs.y.p, e->dobs.z.p, e->dobs.cart_off.p};
 }
 
@@ -58,7 +54,7 @@ int build_pairs(jk_engine* e) {
       cls[pair_class(la, lb)].la = la;
       cls[pair_class(la, lb)].lb = lb;
     }
-  std::vector<double> pp_p, pp_x, pp_y, pp_z, pp_K;
+  std::vector<double> pp_p, pp_x, pp_y, pp_z, pp_K, pp_a;
   for (int i = 0; i < hb.nshell; ++i)
     for (int j = 0; j < hb.nshell; ++j) {
       const int li = hb.l[i], lj = hb.l[j];
@@ -79,6 +75,7 @@ int build_pairs(jk_engine* e) {
           pp_y.push_back((al * A[1] + be * B[1]) / p);
           pp_z.push_back((al * A[2] + be * B[2]) / p);
           pp_K.push_back(K);
+          pp_a.push_back(al);
           ++cnt;
         }
       if (cnt == 0) continue;  // every primitive product vanishes: the pair cannot contribute
@@ -94,6 +91,7 @@ int build_pairs(jk_engine* e) {
   if (st == cudaSuccess) st = e->pp_y.upload(pp_y, s);
   if (st == cudaSuccess) st = e->pp_z.upload(pp_z, s);
   if (st == cudaSuccess) st = e->pp_K.upload(pp_K, s);
+  if (st == cudaSuccess) st = e->pp_a.upload(pp_a, s);
   if (st != cudaSuccess) return check_cuda(e, st, "upload primitive pairs");
 
   // Schwarz bounds on the GPU, class by class

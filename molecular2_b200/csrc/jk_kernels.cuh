@@ -49,8 +49,8 @@ constexpr int UNROLL_LIMIT = 100;
 // over primitive pairs.  out[((ia*NB+ib)*NC+ic)*ND+id].
 template <int LA, int LB, int LC, int LD>
 __device__ __forceinline__ void quartet_cart(const PrimView& pp, int b0, int nb, double Ax, double Ay, double Az,
-                                             double Bx, double By, double Bz, int k0, int nk, double Cx, double Cy,
-                                             double Cz, double Dx, double Dy, double Dz,
+                                             double Bx, double By, double Bz, const PrimView& kp, int k0, int nk,
+                                             double Cx, double Cy, double Cz, double Dx, double Dy, double Dz,
                                              const double* __restrict__ boys_tab, double* out) {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   constexpr int LAB = LA + LB, LCD = LC + LD, L = LAB + LCD;
@@ -67,8 +67,8 @@ __device__ __forceinline__ void quartet_cart(const PrimView& pp, int b0, int nb,
     md_E1<LA, LB>(Py - Ay, Py - By, oo2p, ey);
     md_E1<LA, LB>(Pz - Az, Pz - Bz, oo2p, ez);
     for (int ik = k0; ik < k0 + nk; ++ik) {
-      const double q = __ldg(pp.p + ik), Qx = __ldg(pp.x + ik), Qy = __ldg(pp.y + ik), Qz = __ldg(pp.z + ik);
-      const double Kcd = __ldg(pp.K + ik);
+      const double q = __ldg(kp.p + ik), Qx = __ldg(kp.x + ik), Qy = __ldg(kp.y + ik), Qz = __ldg(kp.z + ik);
+      const double Kcd = __ldg(kp.K + ik);
       E1<LC, LD> fx, fy, fz;
       const double oo2q = 0.5 / q;
       md_E1<LC, LD>(Qx - Cx, Qx - Dx, oo2q, fx);
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(128) k_jk_direct(const JKParams P) {
     if (dn * Qab * Qcd < P.precision) continue;
     ++cnt;
     double eri[NA * NB * NC * ND];
-    quartet_cart<LA, LB, LC, LD>(P.pp, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.ket.prim_off[kl], P.ket.nprim[kl],
+    quartet_cart<LA, LB, LC, LD>(P.pp, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.pp, P.ket.prim_off[kl], P.ket.nprim[kl],
                                  P.sh.x[c], P.sh.y[c], P.sh.z[c], P.sh.x[d], P.sh.y[d], P.sh.z[d], P.boys, eri);
     const double deg = ((a == b) ? 1.0 : 2.0) * ((c == d) ? 1.0 : 2.0) * ((P.same_class && kl == bra) ? 1.0 : 2.0);
     const int c0 = P.sh.coff[c], d0 = P.sh.coff[d];
@@ -353,7 +353,8 @@ __global__ void __launch_bounds__(64) k_schwarz(const SchwarzParams P) {
   double eri[NA * NB * NA * NB];
   const int p0 = P.pairs.prim_off[i], np = P.pairs.nprim[i];
   const double Ax = P.sh.x[a], Ay = P.sh.y[a], Az = P.sh.z[a], Bx = P.sh.x[b], By = P.sh.y[b], Bz = P.sh.z[b];
-  quartet_cart<LA, LB, LA, LB>(P.pp, p0, np, Ax, Ay, Az, Bx, By, Bz, p0, np, Ax, Ay, Az, Bx, By, Bz, P.boys, eri);
+  quartet_cart<LA, LB, LA, LB>(P.pp, p0, np, Ax, Ay, Az, Bx, By, Bz, P.pp, p0, np, Ax, Ay, Az, Bx, By, Bz, P.boys,
+                               eri);
   const int pa = P.pure[a], pb = P.pure[b];
   const int ma = pa ? 2 * LA + 1 : NA, mb = pb ? 2 * LB + 1 : NB;
   double m = 0.0;
@@ -387,6 +388,9 @@ __global__ void __launch_bounds__(64) k_schwarz(const SchwarzParams P) {
     }
   P.Qout[i] = sqrt(m);
 }
+
+struct PairClassDev;
+PairView view(const PairClassDev& c);
 
 // per-translation-unit launchers (jk_cls_*.cu); A, B are pair-class ids
 void launch_jk_bra_s(int A, int B, const JKParams& P, dim3 grid, cudaStream_t s);   // A in {0,1,2}

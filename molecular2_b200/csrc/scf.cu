@@ -1,0 +1,425 @@
+// RHF SCF driver with every n x n quantity resident in HBM: the caller of the
+// J/K engine, restated from molecular2
+//   SCF::rhf                        src/scf.cpp:90-185
+//   SCF::calcE / calcErr            src/scf.cpp:29-58
+//   DIISEngine::compute / solve     src/diis.cpp:22-116
+//   Fock::makeFock / addDiis / average / transform / diagonalise / makeDens
+//                                   src/fockbuild.cpp:176-222, src/fock.cpp:124-244
+// Linear algebra: cuSOLVER syevd (S^-1/2 once, the Fock eigenproblem every
+// iteration), cuBLAS GEMM/dot/nrm2; only the <= (maxdiis+1)^2 DIIS system is
+// solved on the host (full-pivot LU with its rank, as Eigen::FullPivLU).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace m2 {
+
+namespace {
+
+struct Gpu {
+  jk_engine* e;
+  cudaStream_t s;
+  int n;
+  const double one = 1.0, zero = 0.0, mone = -1.0;
+
+  // C = alpha op(A) op(B) + beta C, all n x n unless k given
+  bool gemm(bool ta, bool tb, int m, int nn, int k, double alpha, const double* A, int lda, const double* B, int ldb,
+            double beta, double* C, int ldc) {
+    return cublasDgemm(e->cublas, ta ? CUBLAS_OP_T : CUBLAS_OP_N, tb ? CUBLAS_OP_T : CUBLAS_OP_N, m, nn, k, &alpha,
+                       A, lda, B, ldb, &beta, C, ldc) == CUBLAS_STATUS_SUCCESS;
+  }
+  bool mm(bool ta, bool tb, const double* A, const double* B, double* C, double alpha = 1.0, double beta = 0.0) {
+    return gemm(ta, tb, n, n, n, alpha, A, n, B, n, beta, C, n);
+  }
+  bool axpy(double a, const double* x, double* y, size_t len) {
+    return cublasDaxpy(e->cublas, (int)len, &a, x, 1, y, 1) == CUBLAS_STATUS_SUCCESS;
+  }
+  bool copy(const double* x, double* y, size_t len) {
+    return cudaMemcpyAsync(y, x, len * sizeof(double), cudaMemcpyDeviceToDevice, s) == cudaSuccess;
+  }
+  bool scal(double a, double* x, size_t len) {
+    return cublasDscal(e->cublas, (int)len, &a, x, 1) == CUBLAS_STATUS_SUCCESS;
+  }
+  double dot(const double* x, const double* y, size_t len) {
+    double r = 0.0;
+    cublasDdot(e->cublas, (int)len, x, 1, y, 1, &r);  // host pointer mode: synchronous
+    return r;
+  }
+  double nrm2(const double* x, size_t len) {
+    double r = 0.0;
+    cublasDnrm2(e->cublas, (int)len, x, 1, &r);
+    return r;
+  }
+};
+
+// Eigen::FullPivLU-style solve with rank (threshold eps * size * max pivot).
+void full_piv_solve(std::vector<double> A, int N, std::vector<double> b, std::vector<double>& x, int& rank) {
+  std::vector<int> rp(N), cp(N);
+  for (int i = 0; i < N; ++i) rp[i] = cp[i] = i;
+  auto a = [&](int i, int j) -> double& { return A[(size_t)i * N + j]; };
+  double maxpiv = 0.0;
+  rank = 0;
+  for (int k = 0; k < N; ++k) {
+    int pi = k, pj = k;
+    double best = -1.0;
+    for (int i = k; i < N; ++i)
+      for (int j = k; j < N; ++j)
+        if (std::fabs(a(i, j)) > best) {
+          best = std::fabs(a(i, j));
+          pi = i;
+          pj = j;
+        }
+    if (k == 0) maxpiv = best;
+    if (best <= maxpiv * 2.220446049250313e-16 * N || best == 0.0) break;
+    ++rank;
+    if (pi != k) {
+      for (int j = 0; j < N; ++j) std::swap(a(k, j), a(pi, j));
+      std::swap(b[k], b[pi]);
+      std::swap(rp[k], rp[pi]);
+    }
+    if (pj != k) {
+      for (int i = 0; i < N; ++i) std::swap(a(i, k), a(i, pj));
+      std::swap(cp[k], cp[pj]);
+    }
+    for (int i = k + 1; i < N; ++i) {
+      double f = a(i, k) / a(k, k);
+      if (f == 0.0) continue;
+      for (int j = k; j < N; ++j) a(i, j) -= f * a(k, j);
+      b[i] -= f * b[k];
+    }
+  }
+  std::vector<double> y(N, 0.0);
+  for (int i = rank - 1; i >= 0; --i) {
+    double s = b[i];
+    for (int j = i + 1; j < rank; ++j) s -= a(i, j) * y[j];
+    y[i] = s / a(i, i);
+  }
+  x.assign(N, 0.0);
+  for (int i = 0; i < N; ++i) x[cp[i]] = y[i];
+}
+
+struct Diis {  // DIISEngine (src/diis.cpp) with error vectors in HBM
+  int max = 8;
+  bool use = true;
+  std::vector<DevBuf<double>*> errs;
+  std::vector<double> lastB{0.0};
+  int lastB_dim = 1;
+  ~Diis() {
+    for (auto* p : errs) delete p;
+  }
+
+  static std::vector<double> solve(const std::vector<double>& B, int dim, int start) {
+    const int size = dim - start;
+    double norm = 1.0;
+    if (B[(size_t)start * dim + start] > 1e-10) norm = 1.0 / B[(size_t)start * dim + start];
+    std::vector<double> nB((size_t)size * size, 0.0);
+    for (int i = 0; i < size - 1; ++i) {
+      for (int j = i; j < size - 1; ++j)
+        nB[(size_t)i * size + j] = nB[(size_t)j * size + i] = norm * B[(size_t)(i + start) * dim + j + start];
+      nB[(size_t)i * size + size - 1] = nB[(size_t)(size - 1) * size + i] = -1.0;
+    }
+    nB[(size_t)(size - 1) * size + size - 1] = 0.0;
+    std::vector<double> w(size, 0.0), x;
+    w[size - 1] = -1.0;
+    int rank = 0;
+    full_piv_solve(nB, size, w, x, rank);
+    x.push_back((double)rank);
+    return x;
+  }
+
+  std::vector<double> compute(Gpu& g, const double* err, size_t len) {
+    std::vector<double> weights;
+    const int it = (int)errs.size() + 1;
+    if (!use) return weights;
+    if (it > max) {
+      delete errs.front();
+      errs.erase(errs.begin());
+    }
+    auto* nb = new DevBuf<double>();
+    nb->alloc(len);
+    g.copy(err, nb->p, len);
+    errs.push_back(nb);
+    if (it == 1) {
+      lastB.assign(1, g.dot(nb->p, nb->p, len));
+      lastB_dim = 1;
+    }
+    if (it > 1) {
+      const int lim = std::min(it, max), dim = lim + 1;
+      std::vector<double> B((size_t)dim * dim, 0.0);
+      const int start = it > lim ? 1 : 0;
+      for (int i = 0; i < lim - 1; ++i) {
+        for (int j = i; j < lim - 1; ++j)
+          B[(size_t)i * dim + j] = B[(size_t)j * dim + i] = lastB[(size_t)(i + start) * lastB_dim + j + start];
+        B[(size_t)lim * dim + i] = B[(size_t)i * dim + lim] = -1.0;
+      }
+      for (int i = 0; i < lim; ++i) {
+        double v = g.dot(errs[i]->p, errs[lim - 1]->p, len);
+        B[(size_t)(lim - 1) * dim + i] = B[(size_t)i * dim + lim - 1] = v;
+      }
+      B[(size_t)lim * dim + lim - 1] = B[(size_t)(lim - 1) * dim + lim] = -1.0;
+      lastB = B;
+      lastB_dim = dim;
+      weights = solve(B, dim, 0);
+      int rank = (int)weights.back();
+      int st = 1;
+      while (rank < (lim - st + 1) && st < lim) {
+        weights = solve(B, dim, st++);
+        rank = (int)weights.back();
+      }
+      weights.resize(weights.size() - 2);
+    }
+    return weights;
+  }
+};
+
+}  // namespace
+
+int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
+  const int n = e->obs.n_final, nocc = o->nocc;
+  const size_t nn = (size_t)n * n;
+  if (nocc <= 0 || nocc > n) return set_error(e, JK_ERR_ARG, "scf: nocc out of range");
+  if (o->df && !e->df.ready) {
+    int rc = df_setup(e);
+    if (rc) return rc;
+  }
+  cudaStream_t s = e->stream;
+  cublasSetStream(e->cublas, s);
+  Gpu g{e, s, n};
+  DevBuf<double> S, T, V, H, X, F, Fm, Finc, D, Dd, Dold, C, W, eps, J, K, t1, t2, err, work;
+  DevBuf<int> info;
+  cudaError_t st = cudaSuccess;
+  for (auto* b : {&S, &T, &V, &H, &X, &F, &Fm, &Finc, &D, &Dd, &Dold, &C, &W, &J, &K, &t1, &t2, &err})
+    if (st == cudaSuccess) st = b->alloc(nn);
+  if (st == cudaSuccess) st = eps.alloc(n);
+  if (st == cudaSuccess) st = info.alloc(1);
+  if (st != cudaSuccess) return check_cuda(e, st, "scf allocation");
+  int rc = one_body_device(e, S.p, T.p, V.p, s);
+  if (rc) return rc;
+  g.copy(T.p, H.p, nn);
+  g.axpy(1.0, V.p, H.p, nn);
+  // syevd workspace
+  int lwork = 0;
+  cusolverDnDsyevd_bufferSize(e->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, W.p, n, eps.p, &lwork);
+  if ((st = work.alloc(std::max(lwork, 1))) != cudaSuccess) return check_cuda(e, st, "syevd workspace");
+  auto syev = [&](const double* A, double* vecs, double* vals) -> bool {
+    g.copy(A, vecs, nn);
+    return cusolverDnDsyevd(e->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, vecs, n, vals, work.p,
+                            lwork, info.p) == CUSOLVER_STATUS_SUCCESS;
+  };
+  // S^-1/2 = U lambda^-1/2 U^T (Fock::formOrthog, src/fock.cpp:124-142)
+  std::vector<double> lam(n);
+  if (!syev(S.p, W.p, eps.p)) return set_error(e, JK_ERR_CUDA, "syevd(S)");
+  cudaMemcpyAsync(lam.data(), eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  for (int i = 0; i < n; ++i) {
+    if (!(lam[i] > 0.0)) return set_error(e, JK_ERR_ARG, "overlap matrix is not positive definite");
+    lam[i] = 1.0 / std::sqrt(lam[i]);
+  }
+  g.copy(W.p, t1.p, nn);
+  {
+    DevBuf<double> dl;
+    dl.upload(lam, s);
+    cublasDdgmm(e->cublas, CUBLAS_SIDE_RIGHT, n, n, t1.p, n, dl.p, 1, t1.p, n);  // U diag
+    g.mm(false, true, t1.p, W.p, X.p);                                              // (U diag) U^T
+    cudaStreamSynchronize(s);
+  }
+  double jk_ms = 0.0;
+  int builds = 0;
+  const double enuc = o->enuc;
+  // state of Fock (src/fock.cpp:32-74)
+  bool started_incremental = false, reset_incremental = false, have_dens = false;
+  double next_reset = 0.0, rms_error = 1.0;
+  const double incremental_threshold = 1e-5;
+  int last_reset = 0, fock_iter = 0;
+  const int MAX = o->maxdiis > 0 ? o->maxdiis : 8;
+  std::vector<DevBuf<double>*> focks;
+  Diis diis;
+  diis.max = MAX;
+  diis.use = o->diis != 0;
+  auto transform = [&](const double* Fa) {  // Fm = X^T F X
+    g.mm(false, false, Fa, X.p, t1.p);
+    g.mm(true, false, X.p, t1.p, Fm.p);
+  };
+  auto diagonalise = [&]() -> bool {
+    if (!syev(Fm.p, W.p, eps.p)) return false;
+    return g.mm(false, false, X.p, W.p, C.p);
+  };
+  auto make_dens = [&]() {
+    if (have_dens) {
+      g.copy(D.p, Dd.p, nn);
+      g.scal(-1.0, Dd.p, nn);
+    }
+    g.gemm(false, true, n, n, nocc, 2.0, C.p, n, C.p, n, 0.0, D.p, n);
+    if (!have_dens)
+      g.copy(D.p, Dd.p, nn);
+    else
+      g.axpy(1.0, D.p, Dd.p, nn);
+    have_dens = true;
+  };
+  auto jk = [&](const double* P, double* G) -> int {  // G = J - 1/2 K (direct) or 2J - K (DF, w.r.t. C)
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+    int rc2;
+    if (o->df) {
+      rc2 = df_jk_device(e, C.p, nocc, o->prec_mode, J.p, K.p, s);
+      if (!rc2) {
+        g.copy(J.p, G, nn);
+        g.scal(2.0, G, nn);
+        g.axpy(-1.0, K.p, G, nn);
+      }
+    } else {
+      rc2 = direct_jk_device(e, P, o->precision, 1.0, J.p, K.p, s);
+      if (!rc2) {
+        g.copy(J.p, G, nn);
+        g.axpy(-0.5, K.p, G, nn);
+      }
+    }
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    jk_ms += ms;
+    ++builds;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return rc2;
+  };
+  auto make_fock = [&]() -> int {
+    if (!o->df) {
+      g.copy(Finc.p, F.p, nn);
+      if (!started_incremental && rms_error < incremental_threshold) {
+        started_incremental = true;
+        reset_incremental = false;
+        next_reset = rms_error / 1e1;
+        last_reset = fock_iter - 1;
+      }
+      if (reset_incremental || !started_incremental) {
+        g.copy(H.p, F.p, nn);
+        g.copy(D.p, Dd.p, nn);
+      }
+      if (reset_incremental && started_incremental) {
+        reset_incremental = false;
+        last_reset = fock_iter;
+        next_reset = rms_error / 1e1;
+      }
+      int rc2 = jk(Dd.p, t2.p);
+      if (rc2) return rc2;
+      g.axpy(1.0, t2.p, F.p, nn);
+      g.copy(F.p, Finc.p, nn);
+    } else {
+      int rc2 = jk(nullptr, t2.p);
+      if (rc2) return rc2;
+      g.copy(H.p, F.p, nn);
+      g.axpy(1.0, t2.p, F.p, nn);
+    }
+    if (o->diis) {
+      if (fock_iter >= MAX) {
+        delete focks.front();
+        focks.erase(focks.begin());
+      }
+      auto* f = new DevBuf<double>();
+      f->alloc(nn);
+      g.copy(F.p, f->p, nn);
+      focks.push_back(f);
+      ++fock_iter;
+    }
+    return JK_OK;
+  };
+  auto calc_err = [&]() {  // X^T (F D S - S D F) X
+    g.mm(false, false, D.p, S.p, t1.p);
+    g.mm(false, false, F.p, t1.p, err.p);
+    g.mm(false, false, D.p, F.p, t1.p);
+    g.mm(false, false, S.p, t1.p, err.p, -1.0, 1.0);
+    g.mm(false, false, err.p, X.p, t1.p);
+    g.mm(true, false, X.p, t1.p, err.p);
+  };
+  double energy = 0.0, last_energy = 0.0;
+  auto calc_e = [&]() {  // 1/2 tr(D (H + F)) + Enuc
+    last_energy = energy;
+    g.copy(H.p, t1.p, nn);
+    g.axpy(1.0, F.p, t1.p, nn);
+    energy = 0.5 * g.dot(D.p, t1.p, nn) + enuc;
+  };
+  auto average = [&](const std::vector<double>& w) {
+    if (o->diis && fock_iter > 2) {
+      const int off = (int)focks.size() - (int)w.size();
+      cudaMemsetAsync(F.p, 0, nn * sizeof(double), s);
+      for (int i = off; i < (int)focks.size(); ++i) g.axpy(w[i - off], focks[i]->p, F.p, nn);
+    }
+  };
+  auto cleanup = [&]() {
+    for (auto* f : focks) delete f;
+  };
+  // guess (Fock::transform(true)): core Hamiltonian, or a caller-supplied AO Fock
+  if (o->guess_fock) {
+    cudaMemcpyAsync(F.p, o->guess_fock, nn * sizeof(double), cudaMemcpyHostToDevice, s);
+  } else {
+    g.copy(H.p, F.p, nn);
+  }
+  g.copy(F.p, Finc.p, nn);
+  transform(F.p);
+  if (!diagonalise()) return cleanup(), set_error(e, JK_ERR_CUDA, "syevd(F)");
+  make_dens();
+  g.copy(D.p, Dold.p, nn);
+  if ((rc = make_fock())) return cleanup(), rc;
+  calc_err();
+  std::vector<double> weights = diis.compute(g, err.p, nn);
+  calc_e();
+  average(weights);
+  transform(F.p);
+  int it = 1;
+  bool converged = false;
+  double dd = 0.0, delta = 0.0;
+  while (!converged && it < o->maxiter) {
+    if (!diagonalise()) return cleanup(), set_error(e, JK_ERR_CUDA, "syevd(F)");
+    make_dens();
+    g.copy(D.p, t1.p, nn);
+    g.axpy(-1.0, Dold.p, t1.p, nn);
+    dd = g.nrm2(t1.p, nn);
+    g.copy(D.p, Dold.p, nn);
+    if ((rc = make_fock())) return cleanup(), rc;
+    calc_err();
+    rms_error = g.nrm2(err.p, nn) / (double)nn;
+    if (rms_error < next_reset || it - last_reset > 8) reset_incremental = true;
+    if (it > 2) weights = diis.compute(g, err.p, nn);
+    calc_e();
+    delta = std::fabs(energy - last_energy);
+    if (it > 2) average(weights);
+    transform(F.p);
+    converged = dd < o->densconverge && delta < o->enconverge;
+    ++it;
+  }
+  if (!diagonalise()) return cleanup(), set_error(e, JK_ERR_CUDA, "syevd(F)");
+  st = cudaStreamSynchronize(s);
+  cleanup();
+  if (st != cudaSuccess) return check_cuda(e, st, "scf");
+  r->energy = energy;
+  r->iterations = it;
+  r->converged = converged ? 1 : 0;
+  r->jk_builds = builds;
+  r->jk_ms = jk_ms;
+  r->last_delta_e = delta;
+  r->last_delta_d = dd;
+  if (o->out_density) cudaMemcpy(o->out_density, D.p, nn * sizeof(double), cudaMemcpyDeviceToHost);
+  if (o->out_coeffs) cudaMemcpy(o->out_coeffs, C.p, nn * sizeof(double), cudaMemcpyDeviceToHost);
+  if (o->out_eps) cudaMemcpy(o->out_eps, eps.p, n * sizeof(double), cudaMemcpyDeviceToHost);
+  r->total_ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+  return converged ? JK_OK : JK_ERR_NOT_CONVERGED;
+}
+
+}  // namespace m2
+
+extern "C" int jk_scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
+  if (!e || !o || !r) return JK_ERR_ARG;
+  std::memset(r, 0, sizeof(*r));
+  return m2::scf_rhf(e, o, r);
+}

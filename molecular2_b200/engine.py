@@ -37,7 +37,26 @@ SIGNATURES = {
     "jk_direct": (_I, [_P, _P, _D, _D, _P, _P]),
     "jk_direct_device": (_I, [_P, _P, _D, _D, _P, _P, _P]),
     "jk_last_quartets": (ctypes.c_longlong, [_P]),
+    "jk_eri3": (_I, [_P, _P]),
+    "jk_eri2": (_I, [_P, _P]),
+    "jk_df_setup": (_I, [_P]),
+    "jk_df": (_I, [_P, _P, _I, _I, _P, _P]),
+    "jk_df_device": (_I, [_P, _P, _I, _I, _P, _P, _P]),
+    "jk_one_body": (_I, [_P, _P, _P, _P]),
+    "jk_scf_rhf": (_I, [_P, _P, _P]),
 }
+
+
+class SCFOptions(ctypes.Structure):
+    """ctypes image of ``jk_scf_options``; defaults are molecular2's (src/ProgramController.cpp:296-307)."""
+    _fields_ = [("nocc", _I), ("df", _I), ("prec_mode", _I), ("maxiter", _I), ("maxdiis", _I), ("diis", _I),
+                ("precision", _D), ("enconverge", _D), ("densconverge", _D), ("enuc", _D),
+                ("guess_fock", _P), ("out_density", _P), ("out_coeffs", _P), ("out_eps", _P)]
+
+
+class SCFResult(ctypes.Structure):
+    _fields_ = [("energy", _D), ("iterations", _I), ("converged", _I), ("jk_builds", _I), ("jk_ms", _D),
+                ("total_ms", _D), ("last_delta_e", _D), ("last_delta_d", _D)]
 
 
 class JKError(RuntimeError):
@@ -130,6 +149,64 @@ class IntegralEngine:
         self._check(self.lib.jk_direct_device(self.h, ctypes.c_void_p(dD), precision, multiplier,
                                               ctypes.c_void_p(dJ), ctypes.c_void_p(dK),
                                               ctypes.c_void_p(stream) if stream else None))
+
+    # -- density fitting -----------------------------------------------------
+    def compute_eris_3index(self):
+        """(P|mn) in molecular2's packed layout: (n(n+1)/2) x naux, column-major."""
+        n = self.n
+        T = np.zeros((n * (n + 1) // 2, self.naux), order="F")
+        self._check(self.lib.jk_eri3(self.h, _p(T)))
+        return T
+
+    def compute_eris_2index(self):
+        V = np.zeros((self.naux, self.naux), order="F")
+        self._check(self.lib.jk_eri2(self.h, _p(V)))
+        return V
+
+    def df_setup(self):
+        self._check(self.lib.jk_df_setup(self.h))
+
+    def jk_df(self, Cocc, prec_mode=0):
+        """J, K with respect to Cocc Cocc^T (compute_2body_fock_df)."""
+        n = self.n
+        C = np.asfortranarray(Cocc, dtype=np.float64)
+        J = np.zeros((n, n), order="F")
+        K = np.zeros((n, n), order="F")
+        self._check(self.lib.jk_df(self.h, _p(C), C.shape[1], prec_mode, _p(J), _p(K)))
+        return J, K
+
+    def jk_df_device(self, dC, nocc, dJ, dK, prec_mode=0, stream=None):
+        self._check(self.lib.jk_df_device(self.h, ctypes.c_void_p(dC), nocc, prec_mode, ctypes.c_void_p(dJ),
+                                          ctypes.c_void_p(dK), ctypes.c_void_p(stream) if stream else None))
+
+    # -- one-body and SCF ------------------------------------------------------
+    def one_body(self):
+        n = self.n
+        S, T, V = (np.zeros((n, n), order="F") for _ in range(3))
+        self._check(self.lib.jk_one_body(self.h, _p(S), _p(T), _p(V)))
+        return S, T, V
+
+    def scf_rhf(self, nocc, enuc, df=False, prec_mode=0, maxiter=40, maxdiis=8, diis=True, precision=1e-12,
+                enconverge=1e-7, densconverge=1e-4, guess_fock=None, want=False):
+        """SCF::rhf on the device; returns (SCFResult, extras dict)."""
+        n = self.n
+        o = SCFOptions()
+        o.nocc, o.df, o.prec_mode, o.maxiter, o.maxdiis, o.diis = nocc, int(df), prec_mode, maxiter, maxdiis, int(diis)
+        o.precision, o.enconverge, o.densconverge, o.enuc = precision, enconverge, densconverge, enuc
+        keep = []
+        if guess_fock is not None:
+            gf = np.asfortranarray(guess_fock, dtype=np.float64)
+            keep.append(gf)
+            o.guess_fock = gf.ctypes.data
+        extras = {}
+        if want:
+            extras = {"D": np.zeros((n, n), order="F"), "C": np.zeros((n, n), order="F"), "eps": np.zeros(n)}
+            o.out_density, o.out_coeffs, o.out_eps = (extras[k].ctypes.data for k in ("D", "C", "eps"))
+        r = SCFResult()
+        rc = self.lib.jk_scf_rhf(self.h, ctypes.byref(o), ctypes.byref(r))
+        if rc not in (0, 6):
+            self._check(rc)
+        return r, extras
 
 
 class Fock:
