@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Benchmark of the J/K engine on the (H2O)16 DF-JK workload.
+
+Workload: (H2O)16 water cluster (seeded, 9 A cube), RHF/cc-pVDZ (n = 384)
+with the VDZ-JKFIT fitting basis (naux = 1856), nocc = 80: the density-fitted
+J/K build molecular2 runs every SCF iteration (Fock::formJKdf,
+src/fockbuild.cpp:171-174, 585-660).  A step is one J/K build for the
+converged occupied orbitals; `value` is builds/s with everything resident in
+HBM, `e2e` the same through the host-pointer C entry point (C uploaded, J and
+K downloaded every step).  The whole RHF SCF is timed once per precision
+mode and reported under "scf".
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times molecular2's own algorithm on the host cores: the
+oracle's restatement of compute_2body_fock_df's naive loops (molecular2
+itself needs libint2/Eigen and cannot be built here), on a bounded sample of
+the fitting functions, extrapolated linearly in naux.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DF-JK Fock builds/s, (H2O)16 RHF/cc-pVDZ + VDZ-JKFIT"
+UNIT = "builds/s"
+SEED = 16
+
+
+def workload():
+    from molecular2_b200 import geometry
+    from molecular2_b200.basis import BasisSet
+    mol = geometry.water16(SEED)
+    return mol, BasisSet(mol, "cc-pvdz"), BasisSet(mol, "vdz-jkfit")
+
+
+def config(mol, obs, aux, prec):
+    return {"workload": f"(H2O)16 RHF/cc-pVDZ + VDZ-JKFIT DF-JK build (n={obs.nbf}, naux={aux.nbf}, "
+                        f"nocc={mol.nocc}), seed {SEED}",
+            "precision": prec,
+            "l2": "inputs larger than L2 (FP64 B tensor %.2f GB)" % (obs.nbf ** 2 * aux.nbf * 8 / 1e9),
+            "parallelism": "replicas"}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["hbm_gbs"], d["bf16_tflops"], "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+# ---------------------------------------------------------------- CPU leg
+def cpu_sample(nthreads, target_s=12.0):
+    """Time the naive per-iteration loops of compute_2body_fock_df on a
+    contiguous block of fitting functions; returns (builds/s, sample text)."""
+    import oracle
+    mol, obs, aux = workload()
+    n, naux, nocc = obs.nbf, aux.nbf, mol.nocc
+    rng = np.random.default_rng(0)
+    npair = n * (n + 1) // 2
+    C = np.asfortranarray(rng.normal(size=(n, nocc)))
+
+    def run(nk):
+        B = np.asfortranarray(rng.normal(size=(npair, nk)))
+        t = time.perf_counter()
+        oracle.df_jk(B, C, (0, nk), nthreads=nthreads)
+        return time.perf_counter() - t
+
+    nk = 2
+    t = run(nk)
+    nk = int(max(2, min(naux, nk * target_s / max(t, 1e-3))))
+    t = run(nk)
+    builds_per_s = 1.0 / (t * naux / nk)
+    sample = (f"naive X/K/gamma/J loops of compute_2body_fock_df over {nk} of {naux} fitting functions "
+              f"(synthetic B values), {nthreads} thread(s), {t:.1f} s, extrapolated x{naux / nk:.1f}")
+    return builds_per_s, sample, t
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(nthreads, target_s=2.0)
+    vals = []
+    t0 = time.perf_counter()
+    sample = ""
+    for _ in range(args.steps):
+        v, sample, _ = cpu_sample(nthreads, target_s=4.0)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    v = statistics.median(vals)
+    mol, obs, aux = workload()
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(mol, obs, aux, "fp64"),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index, path):
+        self.path = path
+        self.index = index
+        self.p = None
+        try:
+            self.f = open(path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(index), "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.close()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- GPU leg
+def run_ours(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    from molecular2_b200.engine import IntegralEngine
+    torch.cuda.set_device(local)
+    mol, obs, aux = workload()
+    n, naux, nocc = obs.nbf, aux.nbf, mol.nocc
+    eng = IntegralEngine(obs, aux, device=local)
+    t = time.perf_counter()
+    eng.df_setup()
+    setup_s = time.perf_counter() - t
+    prec_mode = {"fp64": 0, "mixed": 1}[args.precision]
+    # converged orbitals (and the SCF timing) — not part of the timed builds
+    t = time.perf_counter()
+    r64, ex = eng.scf_rhf(nocc, mol.enuc(), df=True, densconverge=1e-6, enconverge=1e-8, want=True)
+    scf64_s = time.perf_counter() - t
+    C = np.ascontiguousarray(ex["C"][:, :nocc])
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    dC = torch.from_numpy(np.ascontiguousarray(C.T)).cuda()        # column-major n x nocc
+    dJ = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    dK = torch.empty((n, n), dtype=torch.float64, device="cuda")
+
+    def step():
+        eng.jk_df_device(dC.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), prec_mode, stream=sh)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local, os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
+                                        else "_work", f"clocks_rank{rank}.csv")) if rank == 0 else None
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    clk = clocks.stop() if clocks else None
+    value = world * args.steps / (ms / 1e3)
+
+    # stage timings of the same builds (CUDA events recorded by the library on `stream`)
+    eng.set_profiling(True)
+    stages = np.zeros(8)
+    nst = 0
+    for _ in range(args.steps):
+        step()
+        s = eng.stage_ms()
+        nst = len(s)
+        stages[:nst] += s
+    eng.set_profiling(False)
+    stages = stages[:nst] / args.steps
+    hbm, bf16, src = peaks()
+    # roofline: the stage that dominates the build
+    B_bytes = n * n * naux * 8
+    X_bytes = n * naux * nocc * 8
+    names = ["X=B.C (cuBLAS DGEMM)", "K=X.X^T (cuBLAS DSYRK)", "gamma (k_gamma)", "J=B.gamma (k_df_J)"]
+    algo = [B_bytes + X_bytes, X_bytes, X_bytes, B_bytes]
+    j = int(np.argmax(stages)) if nst else 0
+    own = 3  # k_df_J (HBM-bound) is the engine's own kernel to report
+    achieved = algo[own] / (stages[own] * 1e-3) / 1e9 if nst > own else None
+    roofline = {"kernel": names[own], "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": (achieved / hbm) if achieved else None, "traffic": None, "peak_source": src,
+                "dominant_stage": names[j] if nst else None,
+                "stage_ms": {names[i]: round(float(stages[i]), 5) for i in range(nst)},
+                "algorithmic_bytes": algo[own]}
+
+    # e2e: host C in (pinned), host J/K out, through the public host-pointer call
+    hC = torch.from_numpy(np.asfortranarray(C)).pin_memory()
+    hJ = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    hK = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    import ctypes
+    lib = eng.lib
+
+    def e2e_step():
+        rc = lib.jk_df(eng.h, ctypes.c_void_p(hC.data_ptr()), nocc, prec_mode, ctypes.c_void_p(hJ.data_ptr()),
+                       ctypes.c_void_p(hK.data_ptr()))
+        if rc:
+            eng._check(rc)
+
+    for _ in range(3):
+        e2e_step()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t
+    if world > 1:
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * nocc * 8,
+           "d2h_bytes_per_step": 2 * n * n * 8}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, sample, _ = cpu_sample(1)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec_mode == 0 else "bf16x3/f32",
+                "data": "synthetic (seeded geometry; basis data from molecular2's library)",
+                "config": config(mol, obs, aux, args.precision), "e2e": e2e, "roofline": roofline,
+                "cpu_baseline": cpu, "clocks": clk, "gpu_launches": 3 * args.steps,
+                "scf": {"fp64": {"energy": r64.energy, "iterations": r64.iterations, "converged": r64.converged,
+                                 "time_s": scf64_s, "jk_ms_total": r64.jk_ms}},
+                "df_setup_s": setup_s}
+        print(json.dumps(line), flush=True)
+    eng.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -106,6 +106,13 @@ int jk_df_setup(jk_engine* e);
 int jk_df(jk_engine* e, const double* Cocc, int nocc, int prec_mode, double* J, double* K);
 int jk_df_device(jk_engine* e, const double* dCocc, int nocc, int prec_mode, double* dJ, double* dK, void* stream);
 
+/* Per-stage device timing of DF builds (CUDA events on the launch stream;
+ * molecular2 only has wall-clock timers, src/logger.cpp:35-40).
+ * jk_stage_ms writes up to nmax stage durations of the last build (ms) and
+ * their count to *nwritten.  FP64 stages are X = B C, K = X X^T, gamma, J. */
+int jk_set_profiling(jk_engine* e, int on);
+int jk_stage_ms(jk_engine* e, float* ms, int nmax, int* nwritten);
+
 /* Overlap, kinetic and nuclear-attraction matrices (point charges of
  * jk_create): IntegralEngine::compute_1body_ints (src/integrals.cpp:394-449). */
 int jk_one_body(jk_engine* e, double* S, double* T, double* V);

@@ -31,11 +31,16 @@ def sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
-def headers():
-    inc = os.path.join(os.path.dirname(HERE), "include")
-    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    hs += [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
-    return hs
+def deps(src, seen=None):
+    """Transitive local #include "..." dependencies of a source file."""
+    import re
+    seen = set() if seen is None else seen
+    for m in re.finditer(r'#include\s+"([^"]+)"', open(src).read()):
+        p = os.path.normpath(os.path.join(os.path.dirname(src), m.group(1)))
+        if os.path.exists(p) and p not in seen:
+            seen.add(p)
+            deps(p, seen)
+    return seen
 
 
 def _obj(src):
@@ -52,11 +57,11 @@ def _compile(src, verbose):
 
 def build(force=False, verbose=False, jobs=None):
     os.makedirs(BUILD, exist_ok=True)
-    hmax = max(os.path.getmtime(h) for h in headers())
     todo = []
     for s in sources():
         o = _obj(s)
-        if force or not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), hmax):
+        newest = max([os.path.getmtime(s)] + [os.path.getmtime(h) for h in deps(s)])
+        if force or not os.path.exists(o) or os.path.getmtime(o) < newest:
             todo.append(s)
     with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count()) as ex:
         for src, rc, out in ex.map(lambda s: _compile(s, verbose), todo):

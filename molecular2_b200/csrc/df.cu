@@ -13,6 +13,7 @@
 //   J[x][y]    = sum_K gamma_K B[x][K][y]     stream X and B once each.
 // B = T L^-T with V = L L^T is formed once per geometry by a strided-batched
 // GEMM with L^-1 (the reference's O(n^2 naux^2) transform at :610-618).
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -247,6 +248,14 @@ int df_setup(jk_engine* e) {
   return JK_OK;
 }
 
+// Record stage boundary k of the DF build when profiling is on.
+static void stage_mark(jk_engine* e, int k, cudaStream_t s) {
+  if (!e->profiling || k >= jk_engine::NSTAGE_EV) return;
+  if (!e->ev[k]) cudaEventCreate(&e->ev[k]);
+  cudaEventRecord(e->ev[k], s);
+  e->nev_used = std::max(e->nev_used, k + 1);
+}
+
 int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ, double* dK, cudaStream_t s) {
   DFState& d = e->df;
   if (!d.ready) return set_error(e, JK_ERR_STATE, "jk_df before jk_df_setup");
@@ -257,18 +266,23 @@ int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ,
   if (st != cudaSuccess) return check_cuda(e, st, "jk_df scratch");
   const double one = 1.0, zero = 0.0;
   cublasSetStream(e->cublas, s);
+  stage_mark(e, 0, s);
   // X (o x n*naux, col-major) = C^T . B   ->  X[x][K][i]
   if (cublasDgemm(e->cublas, CUBLAS_OP_T, CUBLAS_OP_N, nocc, n * naux, n, &one, dC, n, d.B64.p, n, &zero, d.X64.p,
                   nocc) != CUBLAS_STATUS_SUCCESS)
     return set_error(e, JK_ERR_CUDA, "X = B C gemm");
+  stage_mark(e, 1, s);
   // K = X^T X over the (naux*o) inner index
   if (cublasDsyrk(e->cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, naux * nocc, &one, d.X64.p, naux * nocc, &zero,
                   dK, n) != CUBLAS_STATUS_SUCCESS)
     return set_error(e, JK_ERR_CUDA, "K = X X^T syrk");
   const int nb = 256;
   k_sym_from_lower<<<(unsigned)(((size_t)n * n + nb - 1) / nb), nb, 0, s>>>(n, dK);
+  stage_mark(e, 2, s);
   k_gamma<<<naux, 256, 0, s>>>(n, naux, nocc, d.X64.p, dC, d.gamma.p);
+  stage_mark(e, 3, s);
   k_df_J<<<n, 128, 0, s>>>(n, naux, d.B64.p, d.gamma.p, dJ);
+  stage_mark(e, 4, s);
   return check_cuda(e, cudaGetLastError(), "jk_df launch");
 }
 
@@ -368,6 +382,27 @@ int jk_df(jk_engine* e, const double* C, int nocc, int prec_mode, double* J, dou
   if (st == cudaSuccess) st = cudaMemcpyAsync(K, e->Kfinal.p, sizeof(double) * n * n, cudaMemcpyDeviceToHost, e->stream);
   if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
   return check_cuda(e, st, "jk_df download");
+}
+
+int jk_set_profiling(jk_engine* e, int on) {
+  if (!e) return JK_ERR_ARG;
+  e->profiling = on != 0;
+  return JK_OK;
+}
+
+int jk_stage_ms(jk_engine* e, float* ms, int nmax, int* nwritten) {
+  if (!e || !ms || !nwritten) return JK_ERR_ARG;
+  *nwritten = 0;
+  if (!e->profiling || e->nev_used < 2) return set_error(e, JK_ERR_STATE, "profiling off or no build recorded");
+  cudaError_t st = cudaEventSynchronize(e->ev[e->nev_used - 1]);
+  if (st != cudaSuccess) return check_cuda(e, st, "stage events");
+  int k = 0;
+  for (; k + 1 < e->nev_used && k < nmax; ++k) {
+    st = cudaEventElapsedTime(&ms[k], e->ev[k], e->ev[k + 1]);
+    if (st != cudaSuccess) return check_cuda(e, st, "stage events");
+  }
+  *nwritten = k;
+  return JK_OK;
 }
 
 int jk_one_body(jk_engine* e, double* S, double* T, double* V) {

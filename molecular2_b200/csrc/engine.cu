@@ -369,6 +369,8 @@ void jk_destroy(jk_engine* e) {
   if (e->stream) cudaStreamSynchronize(e->stream);
   if (e->cublas) cublasDestroy(e->cublas);
   if (e->cusolver) cusolverDnDestroy(e->cusolver);
+  for (auto& ev : e->ev)
+    if (ev) cudaEventDestroy(ev);
   cudaStream_t s = e->stream;
   delete e;  // frees device buffers
   if (s) cudaStreamDestroy(s);

@@ -118,6 +118,11 @@ struct jk_engine {
   m2::DevBuf<double> Dcart, Jcart, Kcart, Dnorm, Dmax, Dfinal, Jfinal, Kfinal;
   m2::DFState df;
   long long last_quartets = 0;
+  // optional per-stage CUDA-event timing of the DF build (jk_set_profiling)
+  bool profiling = false;
+  static constexpr int NSTAGE_EV = 8;
+  cudaEvent_t ev[NSTAGE_EV] = {};
+  int nev_used = 0;
 };
 
 namespace m2 {

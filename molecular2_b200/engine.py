@@ -44,6 +44,8 @@ SIGNATURES = {
     "jk_df_device": (_I, [_P, _P, _I, _I, _P, _P, _P]),
     "jk_one_body": (_I, [_P, _P, _P, _P]),
     "jk_scf_rhf": (_I, [_P, _P, _P]),
+    "jk_set_profiling": (_I, [_P, _I]),
+    "jk_stage_ms": (_I, [_P, _P, _I, ctypes.POINTER(_I)]),
 }
 
 
@@ -178,6 +180,16 @@ class IntegralEngine:
     def jk_df_device(self, dC, nocc, dJ, dK, prec_mode=0, stream=None):
         self._check(self.lib.jk_df_device(self.h, ctypes.c_void_p(dC), nocc, prec_mode, ctypes.c_void_p(dJ),
                                           ctypes.c_void_p(dK), ctypes.c_void_p(stream) if stream else None))
+
+    def set_profiling(self, on=True):
+        self._check(self.lib.jk_set_profiling(self.h, 1 if on else 0))
+
+    def stage_ms(self, nmax=8):
+        """Device durations (ms) of the stages of the last DF build."""
+        buf = (ctypes.c_float * nmax)()
+        cnt = _I()
+        self._check(self.lib.jk_stage_ms(self.h, ctypes.cast(buf, ctypes.c_void_p), nmax, ctypes.byref(cnt)))
+        return [buf[i] for i in range(cnt.value)]
 
     # -- one-body and SCF ------------------------------------------------------
     def one_body(self):
