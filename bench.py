@@ -8,16 +8,20 @@ src/fockbuild.cpp:171-174, 585-660).  A step is one J/K build for the
 converged occupied orbitals; `value` is builds/s with everything resident in
 HBM, `e2e` the same through the host-pointer C entry point (C uploaded, J and
 K downloaded every step).  The whole RHF SCF is timed once per precision
-mode and reported under "scf".
+mode and reported under "scf" (mixed = split-BF16 tensor-core builds, then
+FP64 builds to convergence), with |dE| between the two.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision mixed|fp64] [--profile]
 
 --impl reference times molecular2's own algorithm on the host cores: the
 oracle's restatement of compute_2body_fock_df's naive loops (molecular2
 itself needs libint2/Eigen and cannot be built here), on a bounded sample of
 the fitting functions, extrapolated linearly in naux.
+--profile runs only the timed builds (no SCF, e2e or CPU leg) for ncu.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -46,7 +50,8 @@ def config(mol, obs, aux, prec):
     return {"workload": f"(H2O)16 RHF/cc-pVDZ + VDZ-JKFIT DF-JK build (n={obs.nbf}, naux={aux.nbf}, "
                         f"nocc={mol.nocc}), seed {SEED}",
             "precision": prec,
-            "l2": "inputs larger than L2 (FP64 B tensor %.2f GB)" % (obs.nbf ** 2 * aux.nbf * 8 / 1e9),
+            "l2": "inputs larger than L2 (B tensor %.2f GB FP64 / %.2f GB split BF16)"
+                  % (obs.nbf ** 2 * aux.nbf * 8 / 1e9, obs.nbf ** 2 * aux.nbf * 4 / 1e9),
             "parallelism": "replicas"}
 
 
@@ -75,9 +80,9 @@ def cpu_sample(nthreads, target_s=12.0):
         oracle.df_jk(B, C, (0, nk), nthreads=nthreads)
         return time.perf_counter() - t
 
-    nk = 2
-    t = run(nk)
-    nk = int(max(2, min(naux, nk * target_s / max(t, 1e-3))))
+    t1, t2 = run(4), run(8)
+    per_k = max((t2 - t1) / 4.0, 1e-6)
+    nk = int(max(4, min(naux, target_s / per_k)))
     t = run(nk)
     builds_per_s = 1.0 / (t * naux / nk)
     sample = (f"naive X/K/gamma/J loops of compute_2body_fock_df over {nk} of {naux} fitting functions "
@@ -90,12 +95,12 @@ def run_reference(args, rank, world):
         return
     nthreads = os.cpu_count() or 1
     for _ in range(args.warmup):
-        cpu_sample(nthreads, target_s=2.0)
+        cpu_sample(nthreads, target_s=1.0)
     vals = []
     t0 = time.perf_counter()
     sample = ""
     for _ in range(args.steps):
-        v, sample, _ = cpu_sample(nthreads, target_s=4.0)
+        v, sample, _ = cpu_sample(nthreads, target_s=3.0)
         vals.append(v)
     wall = time.perf_counter() - t0
     v = statistics.median(vals)
@@ -117,7 +122,6 @@ class Clocks:
 
     def __init__(self, index, path):
         self.path = path
-        self.index = index
         self.p = None
         try:
             self.f = open(path, "w")
@@ -151,6 +155,58 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def roofline_fp64(n, naux, nocc, stages):
+    names = ["X=B.C (cuBLAS DGEMM)", "K=X.X^T (cuBLAS DSYRK)", "gamma (k_gamma)", "J=B.gamma (k_df_J)"]
+    hbm, bf16, src = peaks()
+    B_bytes = n * n * naux * 8
+    own = 3
+    ach = B_bytes / (stages[own] * 1e-3) / 1e9 if len(stages) > own else None
+    return {"kernel": names[own], "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+            "frac": ach / hbm if ach else None, "traffic": None, "peak_source": src,
+            "algorithmic_bytes_per_launch": B_bytes,
+            "stage_ms": {names[i]: round(float(stages[i]), 5) for i in range(len(stages))}}
+
+
+def roofline_mixed(n, naux, nocc, stages):
+    """Dominant kernel of the mixed build and the per-stage bounds.
+    GEMM1 (k_gemm1): reads Bhi+Blo, writes Xhi+Xlo -> HBM-bound;
+    GEMM2 (k_gemm2): 3 split products over the lower-triangle tiles -> tensor;
+    J (k_J_mixed): reads the lower half of Bhi+Blo -> HBM-bound."""
+    hbm, bf16, src = peaks()
+    ldb = ((n + 63) // 64) * 64
+    NP = ((nocc + 15) // 16) * 16
+    nt = (n + 127) // 128
+    b_bytes = 2 * n * naux * ldb * 2
+    x_bytes = 2 * n * naux * NP * 2
+    g1_bytes = b_bytes + x_bytes
+    g1_flops = 3 * 2 * (n * naux) * NP * ldb
+    g2_flops = 3 * 2 * (128 * 128) * (naux * NP) * (nt * (nt + 1) // 2)
+    j_bytes = b_bytes * (n + 1) / (2 * n)
+    names = ["split C + GEMM1 X=B.C (k_gemm1, tcgen05)", "GEMM2 K=X.X^T (k_gemm2, tcgen05)",
+             "J=B.gamma (k_J_mixed)", "finalize (k_finalize_mixed)"]
+    per = []
+    if len(stages) >= 3:
+        per = [{"stage": names[0], "ms": stages[0], "bound": "hbm", "achieved_GBs": g1_bytes / stages[0] / 1e6,
+                "frac_hbm": g1_bytes / stages[0] / 1e6 / hbm, "tflops": g1_flops / stages[0] / 1e9},
+               {"stage": names[1], "ms": stages[1], "bound": "tensor", "tflops": g2_flops / stages[1] / 1e9,
+                "frac_tensor": g2_flops / stages[1] / 1e9 / bf16},
+               {"stage": names[2], "ms": stages[2], "bound": "hbm", "achieved_GBs": j_bytes / stages[2] / 1e6,
+                "frac_hbm": j_bytes / stages[2] / 1e6 / hbm}]
+    dom = int(np.argmax(stages[:3])) if len(stages) >= 3 else 0
+    if dom == 1:
+        ach = g2_flops / stages[1] / 1e9
+        rl = {"kernel": names[1], "bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
+              "frac": ach / bf16, "algorithmic_flops_per_launch": g2_flops}
+    else:
+        byts = g1_bytes if dom == 0 else j_bytes
+        ach = byts / stages[dom] / 1e6 if stages else None
+        rl = {"kernel": names[dom], "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+              "frac": ach / hbm if ach else None, "algorithmic_bytes_per_launch": byts}
+    rl.update({"traffic": None, "peak_source": src, "stages": per,
+               "stage_ms": {names[i]: round(float(stages[i]), 5) for i in range(len(stages))}})
+    return rl
+
+
 # ---------------------------------------------------------------- GPU leg
 def run_ours(args, rank, world, local):
     import torch
@@ -164,16 +220,33 @@ def run_ours(args, rank, world, local):
     eng.df_setup()
     setup_s = time.perf_counter() - t
     prec_mode = {"fp64": 0, "mixed": 1}[args.precision]
-    # converged orbitals (and the SCF timing) — not part of the timed builds
-    t = time.perf_counter()
-    r64, ex = eng.scf_rhf(nocc, mol.enuc(), df=True, densconverge=1e-6, enconverge=1e-8, want=True)
-    scf64_s = time.perf_counter() - t
-    C = np.ascontiguousarray(ex["C"][:, :nocc])
-    stream = torch.cuda.current_stream()
+    scf = {}
+    if args.profile:
+        rng = np.random.default_rng(0)
+        C, _ = np.linalg.qr(rng.normal(size=(n, nocc)))
+    else:
+        # SCF in both modes (not part of the timed builds); the FP64 orbitals feed the builds
+        t = time.perf_counter()
+        r64, ex = eng.scf_rhf(nocc, mol.enuc(), df=True, densconverge=1e-6, enconverge=1e-8, want=True)
+        s64 = time.perf_counter() - t
+        t = time.perf_counter()
+        rmx, _ = eng.scf_rhf(nocc, mol.enuc(), df=True, prec_mode=1, densconverge=1e-6, enconverge=1e-8)
+        smx = time.perf_counter() - t
+        scf = {"fp64": {"energy": r64.energy, "iterations": r64.iterations, "converged": r64.converged,
+                        "time_s": s64, "jk_ms_total": r64.jk_ms},
+               "mixed": {"energy": rmx.energy, "iterations": rmx.iterations, "converged": rmx.converged,
+                         "time_s": smx, "jk_ms_total": rmx.jk_ms, "mixed_builds": rmx.mixed_builds},
+               "abs_dE_mixed_vs_fp64": abs(rmx.energy - r64.energy),
+               "speedup_time": s64 / smx if smx > 0 else None,
+               "convergence": "||dD||_F < 1e-6 and |dE| < 1e-8 Eh, core-Hamiltonian guess"}
+        C = np.ascontiguousarray(ex["C"][:, :nocc])
+    stream = torch.cuda.Stream()
     sh = stream.cuda_stream
-    dC = torch.from_numpy(np.ascontiguousarray(C.T)).cuda()        # column-major n x nocc
-    dJ = torch.empty((n, n), dtype=torch.float64, device="cuda")
-    dK = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    with torch.cuda.stream(stream):
+        dC = torch.from_numpy(np.ascontiguousarray(C.T)).cuda()   # column-major n x nocc
+        dJ = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        dK = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
 
     def step():
         eng.jk_df_device(dC.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), prec_mode, stream=sh)
@@ -183,10 +256,11 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clocks = Clocks(local, os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
-                                        else "_work", f"clocks_rank{rank}.csv")) if rank == 0 else None
+    clocks = None
+    if rank == 0 and not args.profile:
+        outdir = os.path.join(ROOT, "gpurun_out") if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp"
+        clocks = Clocks(local, os.path.join(outdir, f"clocks_rank{rank}.csv"))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
     ev0.record(stream)
     for _ in range(args.steps):
         step()
@@ -200,43 +274,40 @@ def run_ours(args, rank, world, local):
         dist.barrier()
     clk = clocks.stop() if clocks else None
     value = world * args.steps / (ms / 1e3)
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile": True, "ms_per_step": ms / args.steps, "value": value}), flush=True)
+        eng.close()
+        return
 
-    # stage timings of the same builds (CUDA events recorded by the library on `stream`)
+    # per-stage durations of the same builds (events recorded by the library on `stream`)
     eng.set_profiling(True)
-    stages = np.zeros(8)
-    nst = 0
+    acc = None
     for _ in range(args.steps):
         step()
-        s = eng.stage_ms()
-        nst = len(s)
-        stages[:nst] += s
+        s = np.array(eng.stage_ms())
+        acc = s if acc is None else acc + s
     eng.set_profiling(False)
-    stages = stages[:nst] / args.steps
-    hbm, bf16, src = peaks()
-    # roofline: the stage that dominates the build
-    B_bytes = n * n * naux * 8
-    X_bytes = n * naux * nocc * 8
-    names = ["X=B.C (cuBLAS DGEMM)", "K=X.X^T (cuBLAS DSYRK)", "gamma (k_gamma)", "J=B.gamma (k_df_J)"]
-    algo = [B_bytes + X_bytes, X_bytes, X_bytes, B_bytes]
-    j = int(np.argmax(stages)) if nst else 0
-    own = 3  # k_df_J (HBM-bound) is the engine's own kernel to report
-    achieved = algo[own] / (stages[own] * 1e-3) / 1e9 if nst > own else None
-    roofline = {"kernel": names[own], "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": (achieved / hbm) if achieved else None, "traffic": None, "peak_source": src,
-                "dominant_stage": names[j] if nst else None,
-                "stage_ms": {names[i]: round(float(stages[i]), 5) for i in range(nst)},
-                "algorithmic_bytes": algo[own]}
+    stages = list(acc / args.steps)
+    roofline = roofline_mixed(n, naux, nocc, stages) if prec_mode == 1 else roofline_fp64(n, naux, nocc, stages)
+    if prec_mode == 1:
+        J64 = torch.empty_like(dJ)
+        K64 = torch.empty_like(dK)
+        eng.jk_df_device(dC.data_ptr(), nocc, J64.data_ptr(), K64.data_ptr(), 0, stream=sh)
+        step()
+        torch.cuda.synchronize()
+        roofline["max_rel_err_vs_fp64"] = {
+            "J": float((dJ - J64).abs().max() / J64.abs().max()),
+            "K": float((dK - K64).abs().max() / K64.abs().max())}
 
     # e2e: host C in (pinned), host J/K out, through the public host-pointer call
     hC = torch.from_numpy(np.asfortranarray(C)).pin_memory()
     hJ = torch.empty((n, n), dtype=torch.float64).pin_memory()
     hK = torch.empty((n, n), dtype=torch.float64).pin_memory()
-    import ctypes
-    lib = eng.lib
 
     def e2e_step():
-        rc = lib.jk_df(eng.h, ctypes.c_void_p(hC.data_ptr()), nocc, prec_mode, ctypes.c_void_p(hJ.data_ptr()),
-                       ctypes.c_void_p(hK.data_ptr()))
+        rc = eng.lib.jk_df(eng.h, ctypes.c_void_p(hC.data_ptr()), nocc, prec_mode, ctypes.c_void_p(hJ.data_ptr()),
+                           ctypes.c_void_p(hK.data_ptr()))
         if rc:
             eng._check(rc)
 
@@ -252,7 +323,7 @@ def run_ours(args, rank, world, local):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
     e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * nocc * 8,
-           "d2h_bytes_per_step": 2 * n * n * 8}
+           "d2h_bytes_per_step": 2 * n * n * 8, "timing": "host wall clock around synchronous calls"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -260,14 +331,13 @@ def run_ours(args, rank, world, local):
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
 
     if rank == 0:
+        launches = 5 if prec_mode == 1 else 3
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec_mode == 0 else "bf16x3/f32",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec_mode == 0 else "bf16x3->f32",
                 "data": "synthetic (seeded geometry; basis data from molecular2's library)",
                 "config": config(mol, obs, aux, args.precision), "e2e": e2e, "roofline": roofline,
-                "cpu_baseline": cpu, "clocks": clk, "gpu_launches": 3 * args.steps,
-                "scf": {"fp64": {"energy": r64.energy, "iterations": r64.iterations, "converged": r64.converged,
-                                 "time_s": scf64_s, "jk_ms_total": r64.jk_ms}},
+                "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches * args.steps, "scf": scf,
                 "df_setup_s": setup_s}
         print(json.dumps(line), flush=True)
     eng.close()
@@ -279,7 +349,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--profile", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))

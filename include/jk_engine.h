@@ -125,7 +125,9 @@ int jk_one_body(jk_engine* e, double* S, double* T, double* V);
 typedef struct jk_scf_options {
   int nocc;
   int df;                  /* 0 = integral-direct J/K, 1 = density-fitted */
-  int prec_mode;           /* DF only: 0 = FP64 */
+  int prec_mode;           /* DF only: 0 = FP64; 1 = split-BF16 tensor-core builds while
+                              ||D - D_old||_F >= mixed_switch, FP64 builds after that */
+  double mixed_switch;     /* default 1e-5 */
   int maxiter;             /* molecular2 default 40 */
   int maxdiis;             /* default 8 */
   int diis;                /* 1 = on */
@@ -148,6 +150,7 @@ typedef struct jk_scf_result {
   double total_ms;         /* host wall time of the whole call */
   double last_delta_e;
   double last_delta_d;
+  int mixed_builds;        /* J/K builds done in mixed precision */
 } jk_scf_result;
 
 int jk_scf_rhf(jk_engine* e, const jk_scf_options* opt, jk_scf_result* res);

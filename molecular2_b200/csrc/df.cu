@@ -249,7 +249,7 @@ int df_setup(jk_engine* e) {
 }
 
 // Record stage boundary k of the DF build when profiling is on.
-static void stage_mark(jk_engine* e, int k, cudaStream_t s) {
+void stage_mark(jk_engine* e, int k, cudaStream_t s) {
   if (!e->profiling || k >= jk_engine::NSTAGE_EV) return;
   if (!e->ev[k]) cudaEventCreate(&e->ev[k]);
   cudaEventRecord(e->ev[k], s);
@@ -259,6 +259,7 @@ static void stage_mark(jk_engine* e, int k, cudaStream_t s) {
 int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ, double* dK, cudaStream_t s) {
   DFState& d = e->df;
   if (!d.ready) return set_error(e, JK_ERR_STATE, "jk_df before jk_df_setup");
+  if (mode == 1) return df_mixed_device(e, dC, nocc, dJ, dK, s);
   if (mode != 0) return set_error(e, JK_ERR_ARG, "jk_df: unsupported precision mode");
   const int n = e->obs.n_final, naux = d.naux;
   cudaError_t st = d.X64.alloc((size_t)n * naux * nocc);
@@ -381,7 +382,8 @@ int jk_df(jk_engine* e, const double* C, int nocc, int prec_mode, double* J, dou
   st = cudaMemcpyAsync(J, e->Jfinal.p, sizeof(double) * n * n, cudaMemcpyDeviceToHost, e->stream);
   if (st == cudaSuccess) st = cudaMemcpyAsync(K, e->Kfinal.p, sizeof(double) * n * n, cudaMemcpyDeviceToHost, e->stream);
   if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
-  return check_cuda(e, st, "jk_df download");
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_df download");
+  return prec_mode == 1 ? df_mixed_error(e) : JK_OK;
 }
 
 int jk_set_profiling(jk_engine* e, int on) {

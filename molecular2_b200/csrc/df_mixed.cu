@@ -1,0 +1,581 @@
+// Mixed-precision DF J/K on the tcgen05 tensor cores (prec_mode 1).
+//
+// Same contraction as the FP64 path (compute_2body_fock_df, molecular2
+// src/fockbuild.cpp:621-659), with B = Bhi + Blo and C = Chi + Clo split into
+// BF16 pairs and every product formed as hi*hi + hi*lo + lo*hi with FP32
+// accumulation in tensor memory (~16 significant bits per operand):
+//   GEMM1  X[m][i] = sum_y B[m][y] C[y][i],  m = (x,K): persistent kernel over
+//          128-row tiles, TMA -> 4-stage smem ring -> tcgen05.mma (M=128,
+//          N=nocc padded to 16) -> double-buffered TMEM accumulators.  The
+//          epilogue re-splits X into BF16 hi/lo for GEMM2 and accumulates
+//          gamma_K = sum_{x,i} X[x][K][i] C[x][i] (FP64 atomics).
+//   GEMM2  K = X X^T over the naux*nocc index: 128x128 tiles of the lower
+//          triangle, split-K across the SMs, FP32 atomics.
+//   J      J[x][y] = sum_K gamma_K B[x][K][y] over y <= x: HBM-bound stream of
+//          the lower half of B (hi + lo).
+// One warp issues TMA, one issues MMA, four drain TMEM; all waits are bounded
+// and report through an error word instead of hanging.
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include <cudaTypedefs.h>
+
+#include "engine.h"
+#include "tc_gemm.cuh"
+
+namespace m2 {
+using namespace tc;
+
+constexpr int BM = 128;           // MMA / tile rows
+constexpr int BK = 64;            // BF16 elements per 128-byte swizzle row
+constexpr int TILE_A_BYTES = BM * BK * 2;
+constexpr int SMEM_LIMIT = 227 * 1024;
+
+enum : int { ERR_NONE = 0, ERR_WAIT_PRODUCER = 1, ERR_WAIT_MMA = 2, ERR_WAIT_EPILOGUE = 3 };
+
+__device__ __forceinline__ void report(int* err, int code) { atomicCAS(err, 0, code); }
+
+// ---------------------------------------------------------------- GEMM1
+struct G1Params {
+  int M;            // n * naux rows of B
+  int kblocks;      // ldb / 64
+  int nocc;
+  int n, naux;
+  int ntiles;
+  const double* C;  // n x nocc column-major
+  __nv_bfloat16* Xhi;  // [m][NP]
+  __nv_bfloat16* Xlo;
+  double* gamma;
+  int* err;
+};
+
+template <int NP>
+struct G1Layout {
+  static constexpr int B_BYTES = NP * BK * 2;
+  static constexpr int STAGE = 2 * TILE_A_BYTES + 2 * B_BYTES;
+  static constexpr int STAGES = std::min(4, (SMEM_LIMIT - 4096) / STAGE);
+  static constexpr int SMEM = STAGES * STAGE + 1024 /*barriers*/ + 1024 /*alignment*/;
+  static constexpr int ACC_STRIDE = NP <= 128 ? 128 : 256;  // TMEM columns per accumulator buffer
+  static constexpr int TMEM_COLS = 2 * ACC_STRIDE;
+};
+
+template <int NP>
+__global__ void __launch_bounds__(192, 1)
+    k_gemm1(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
+            const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl, const G1Params P) {
+  using Lay = G1Layout<NP>;
+  constexpr int S = Lay::STAGES;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = (uint64_t*)(smem + S * Lay::STAGE);
+  uint64_t* empty = full + S;
+  uint64_t* tfull = empty + S;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* drain = tempty + 2;
+  uint32_t* tmem_slot = (uint32_t*)(drain + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);
+    }
+    mbar_init(drain, 1);
+    fence_barrier_init();
+    prefetch_tmap(&tAh);
+    prefetch_tmap(&tAl);
+    prefetch_tmap(&tBh);
+    prefetch_tmap(&tBl);
+  }
+  if (warp == 0) tmem_alloc(tmem_slot, Lay::TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {  // TMA producer
+      int it = 0, last_s = -1;
+      uint32_t last_par = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < P.ntiles && ok; t += gridDim.x)
+        for (int kb = 0; kb < P.kblocks; ++kb, ++it) {
+          const int s = it % S;
+          const uint32_t j = it / S;
+          if (!mbar_wait(&empty[s], (j & 1) ^ 1)) {
+            report(P.err, ERR_WAIT_PRODUCER);
+            ok = false;
+            break;
+          }
+          uint8_t* st = smem + s * Lay::STAGE;
+          mbar_arrive_expect_tx(&full[s], Lay::STAGE);
+          tma_load_2d(st, &tAh, kb * BK, t * BM, &full[s]);
+          tma_load_2d(st + TILE_A_BYTES, &tAl, kb * BK, t * BM, &full[s]);
+          tma_load_2d(st + 2 * TILE_A_BYTES, &tBh, kb * BK, 0, &full[s]);
+          tma_load_2d(st + 2 * TILE_A_BYTES + Lay::B_BYTES, &tBl, kb * BK, 0, &full[s]);
+          last_s = s;
+          last_par = j & 1;
+        }
+      if (last_s >= 0) mbar_wait(&full[last_s], last_par);  // no copy still in flight at exit
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      constexpr uint32_t idesc = idesc_bf16_f32(BM, NP);
+      int it = 0, lt = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < P.ntiles && ok; t += gridDim.x, ++lt) {
+        const int b = lt & 1;
+        const uint32_t u = lt >> 1;
+        if (!mbar_wait(&tempty[b], (u & 1) ^ 1)) {
+          report(P.err, ERR_WAIT_MMA);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem + b * Lay::ACC_STRIDE;
+        for (int kb = 0; kb < P.kblocks; ++kb, ++it) {
+          const int s = it % S;
+          const uint32_t j = it / S;
+          if (!mbar_wait(&full[s], j & 1)) {
+            report(P.err, ERR_WAIT_MMA);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint8_t* st = smem + s * Lay::STAGE;
+#pragma unroll
+          for (int k = 0; k < BK / 16; ++k) {
+            const uint64_t ah = sdesc_kmajor_sw128(st + k * 32);
+            const uint64_t al = sdesc_kmajor_sw128(st + TILE_A_BYTES + k * 32);
+            const uint64_t bh = sdesc_kmajor_sw128(st + 2 * TILE_A_BYTES + k * 32);
+            const uint64_t bl = sdesc_kmajor_sw128(st + 2 * TILE_A_BYTES + Lay::B_BYTES + k * 32);
+            umma_bf16(d, ah, bh, idesc, (kb > 0 || k > 0) ? 1u : 0u);
+            umma_bf16(d, ah, bl, idesc, 1u);
+            umma_bf16(d, al, bh, idesc, 1u);
+          }
+          umma_commit(&empty[s]);
+        }
+        if (ok) umma_commit(&tfull[b]);
+      }
+      umma_commit(drain);  // every issued MMA has finished before TMEM is freed
+      mbar_wait(drain, 0);
+    }
+  } else {  // epilogue: warps 2..5 drain TMEM lanes 32*(warp%4) ..
+    const int q = warp & 3;
+    int lt = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++lt) {
+      const int b = lt & 1;
+      const uint32_t u = lt >> 1;
+      if (!mbar_wait(&tfull[b], u & 1)) {
+        report(P.err, ERR_WAIT_EPILOGUE);
+        break;
+      }
+      tc_fence_after();
+      float v[NP];
+      const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + b * Lay::ACC_STRIDE;
+#pragma unroll
+      for (int c = 0; c < NP / 16; ++c) tmem_ld16(taddr + c * 16, v + c * 16);
+      tmem_ld_wait();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[b]);
+      const int m = t * BM + 32 * q + lane;
+      if (m < P.M) {
+        const int x = m / P.naux, K = m - x * P.naux;
+        double g = 0.0;
+        for (int i = 0; i < P.nocc; ++i) g += (double)v[i] * P.C[(size_t)i * P.n + x];
+        atomicAdd(P.gamma + K, g);
+        uint4* oh = reinterpret_cast<uint4*>(P.Xhi + (size_t)m * NP);
+        uint4* ol = reinterpret_cast<uint4*>(P.Xlo + (size_t)m * NP);
+#pragma unroll
+        for (int c = 0; c < NP / 8; ++c) {
+          __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const float f = v[c * 8 + e];
+            h[e] = __float2bfloat16_rn(f);
+            l[e] = __float2bfloat16_rn(f - __bfloat162float(h[e]));
+          }
+          oh[c] = *reinterpret_cast<const uint4*>(h);
+          ol[c] = *reinterpret_cast<const uint4*>(l);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, Lay::TMEM_COLS);
+  }
+}
+
+// ---------------------------------------------------------------- GEMM2
+struct G2Params {
+  int n;
+  int kblocks;      // (naux*NP)/64
+  int ntile_n;      // ceil(n/128)
+  int ntiles_u;     // lower-triangle tiles
+  int splits;
+  float* Kt;        // n x n, Kt[y*n + x] = K[x][y] for tile(x) >= tile(y)
+  int* err;
+};
+
+constexpr int G2_STAGE = 4 * TILE_A_BYTES;
+constexpr int G2_STAGES = 3;
+constexpr int G2_SMEM = G2_STAGES * G2_STAGE + 1024 + 1024;
+
+__global__ void __launch_bounds__(192, 1)
+    k_gemm2(const __grid_constant__ CUtensorMap tXh, const __grid_constant__ CUtensorMap tXl, const G2Params P) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = (uint64_t*)(smem + G2_STAGES * G2_STAGE);
+  uint64_t* empty = full + G2_STAGES;
+  uint64_t* tfull = empty + G2_STAGES;
+  uint64_t* drain = tfull + 1;
+  uint32_t* tmem_slot = (uint32_t*)(drain + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // which lower-triangle tile and which slice of the inner index
+  const int tile = blockIdx.x % P.ntiles_u, split = blockIdx.x / P.ntiles_u;
+  int tx = 0, ty = 0;
+  {
+    int r = tile;
+    while (r > tx) {
+      r -= tx + 1;
+      ++tx;
+    }
+    ty = r;
+  }
+  const int kb0 = (int)((long long)P.kblocks * split / P.splits);
+  const int kb1 = (int)((long long)P.kblocks * (split + 1) / P.splits);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < G2_STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&tfull[0], 1);
+    mbar_init(drain, 1);
+    fence_barrier_init();
+    prefetch_tmap(&tXh);
+    prefetch_tmap(&tXl);
+  }
+  if (warp == 0) tmem_alloc(tmem_slot, 128);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const bool have_work = kb1 > kb0;
+
+  if (warp == 0) {
+    if (lane == 0 && have_work) {
+      int last_s = -1;
+      uint32_t last_par = 0;
+      for (int kb = kb0, it = 0; kb < kb1; ++kb, ++it) {
+        const int s = it % G2_STAGES;
+        const uint32_t j = it / G2_STAGES;
+        if (!mbar_wait(&empty[s], (j & 1) ^ 1)) {
+          report(P.err, ERR_WAIT_PRODUCER);
+          break;
+        }
+        uint8_t* st = smem + s * G2_STAGE;
+        mbar_arrive_expect_tx(&full[s], G2_STAGE);
+        tma_load_2d(st, &tXh, kb * BK, tx * BM, &full[s]);
+        tma_load_2d(st + TILE_A_BYTES, &tXl, kb * BK, tx * BM, &full[s]);
+        tma_load_2d(st + 2 * TILE_A_BYTES, &tXh, kb * BK, ty * BM, &full[s]);
+        tma_load_2d(st + 3 * TILE_A_BYTES, &tXl, kb * BK, ty * BM, &full[s]);
+        last_s = s;
+        last_par = j & 1;
+      }
+      if (last_s >= 0) mbar_wait(&full[last_s], last_par);
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && have_work) {
+      constexpr uint32_t idesc = idesc_bf16_f32(BM, BM);
+      bool ok = true;
+      for (int kb = kb0, it = 0; kb < kb1; ++kb, ++it) {
+        const int s = it % G2_STAGES;
+        const uint32_t j = it / G2_STAGES;
+        if (!mbar_wait(&full[s], j & 1)) {
+          report(P.err, ERR_WAIT_MMA);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint8_t* st = smem + s * G2_STAGE;
+#pragma unroll
+        for (int k = 0; k < BK / 16; ++k) {
+          const uint64_t ah = sdesc_kmajor_sw128(st + k * 32);
+          const uint64_t al = sdesc_kmajor_sw128(st + TILE_A_BYTES + k * 32);
+          const uint64_t bh = sdesc_kmajor_sw128(st + 2 * TILE_A_BYTES + k * 32);
+          const uint64_t bl = sdesc_kmajor_sw128(st + 3 * TILE_A_BYTES + k * 32);
+          umma_bf16(tmem, ah, bh, idesc, (it > 0 || k > 0) ? 1u : 0u);
+          umma_bf16(tmem, ah, bl, idesc, 1u);
+          umma_bf16(tmem, al, bh, idesc, 1u);
+        }
+        umma_commit(&empty[s]);
+      }
+      if (ok) umma_commit(&tfull[0]);
+      umma_commit(drain);
+      mbar_wait(drain, 0);
+    }
+  } else if (have_work) {
+    const int q = warp & 3;
+    if (!mbar_wait(&tfull[0], 0)) {
+      report(P.err, ERR_WAIT_EPILOGUE);
+    } else {
+      tc_fence_after();
+      const int x = tx * BM + 32 * q + lane;
+      const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16);
+#pragma unroll 1
+      for (int c = 0; c < BM / 16; ++c) {
+        float v[16];
+        tmem_ld16(taddr + c * 16, v);
+        tmem_ld_wait();
+        if (x < P.n) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const int y = ty * BM + c * 16 + e;
+            if (y < P.n) atomicAdd(P.Kt + (size_t)y * P.n + x, v[e]);
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 128);
+  }
+}
+
+// ---------------------------------------------------------------- small kernels
+// B64[x][K][y] (ld n) -> Bhi/Blo[x][K][y] (ld ldb, zero padded)
+__global__ void k_split_B(size_t rows, int n, int ldb, const double* __restrict__ B, __nv_bfloat16* __restrict__ Bh,
+                          __nv_bfloat16* __restrict__ Bl) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * ldb) return;
+  const size_t r = i / ldb;
+  const int y = (int)(i % ldb);
+  const float f = y < n ? (float)B[r * n + y] : 0.0f;
+  const double dv = y < n ? B[r * n + y] : 0.0;
+  const __nv_bfloat16 h = __float2bfloat16_rn(f);
+  Bh[i] = h;
+  Bl[i] = __float2bfloat16_rn((float)(dv - (double)__bfloat162float(h)));
+}
+
+// C (n x nocc col-major FP64) -> ChiT/CloT[i][y] (NP x ldb, zero padded)
+__global__ void k_split_C(int n, int nocc, int NP, int ldb, const double* __restrict__ C, __nv_bfloat16* Ch,
+                          __nv_bfloat16* Cl) {
+  const int i = blockIdx.y, y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (y >= ldb) return;
+  const double dv = (i < nocc && y < n) ? C[(size_t)i * n + y] : 0.0;
+  const __nv_bfloat16 h = __float2bfloat16_rn((float)dv);
+  Ch[(size_t)i * ldb + y] = h;
+  Cl[(size_t)i * ldb + y] = __float2bfloat16_rn((float)(dv - (double)__bfloat162float(h)));
+}
+
+// J[x][y] += sum_{K in chunk} gamma_K (Bhi + Blo)[x][K][y] for y <= x (8 y per thread)
+__global__ void k_J_mixed(int n, int naux, int ldb, int kchunk, const __nv_bfloat16* __restrict__ Bh,
+                          const __nv_bfloat16* __restrict__ Bl, const double* __restrict__ gamma,
+                          double* __restrict__ J) {
+  const int x = blockIdx.x;
+  const int y0 = threadIdx.x * 8;
+  if (y0 > x) return;
+  const int K0 = blockIdx.y * kchunk, K1 = min(naux, K0 + kchunk);
+  float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const size_t base = (size_t)x * naux * ldb + y0;
+#pragma unroll 4
+  for (int K = K0; K < K1; ++K) {
+    const float g = (float)__ldg(gamma + K);
+    const uint4 hv = __ldg(reinterpret_cast<const uint4*>(Bh + base + (size_t)K * ldb));
+    const uint4 lv = __ldg(reinterpret_cast<const uint4*>(Bl + base + (size_t)K * ldb));
+    const __nv_bfloat16* h = reinterpret_cast<const __nv_bfloat16*>(&hv);
+    const __nv_bfloat16* l = reinterpret_cast<const __nv_bfloat16*>(&lv);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) acc[e] += g * (__bfloat162float(h[e]) + __bfloat162float(l[e]));
+  }
+#pragma unroll
+  for (int e = 0; e < 8; ++e)
+    if (y0 + e <= x && y0 + e < n) atomicAdd(J + (size_t)(y0 + e) * n + x, (double)acc[e]);
+}
+
+// J: mirror the lower triangle; K: assemble from the lower-triangle tiles of Kt
+__global__ void k_finalize_mixed(int n, const float* __restrict__ Kt, double* __restrict__ J, double* __restrict__ K) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)n * n) return;
+  const int i = (int)(idx % n), j = (int)(idx / n);  // element (i, j), column-major
+  const int ti = i / BM, tj = j / BM;
+  K[idx] = (ti >= tj) ? (double)Kt[(size_t)j * n + i] : (double)Kt[(size_t)i * n + j];
+  if (i < j) J[idx] = J[(size_t)i * n + j];
+}
+__global__ void k_zero_upper(int n, double* J) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)n * n) return;
+  if ((int)(idx % n) < (int)(idx / n)) J[idx] = 0.0;
+}
+
+// ---------------------------------------------------------------- host
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// 2-D BF16 tensor map: inner extent `cols` (contiguous), `rows`, box box_cols x box_rows, 128B swizzle.
+static bool make_map(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint32_t box_cols,
+                     uint32_t box_rows) {
+  auto enc = get_encode();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {cols, rows};
+  cuuint64_t strides[1] = {cols * 2};
+  cuuint32_t box[2] = {box_cols, box_rows};
+  cuuint32_t es[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int NP>
+static cudaError_t launch_g1(const CUtensorMap* m, const G1Params& P, int grid, cudaStream_t s) {
+  using Lay = G1Layout<NP>;
+  cudaError_t st = cudaFuncSetAttribute(k_gemm1<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::SMEM);
+  if (st != cudaSuccess) return st;
+  k_gemm1<NP><<<grid, 192, Lay::SMEM, s>>>(m[0], m[1], m[2], m[3], P);
+  return cudaGetLastError();
+}
+
+static cudaError_t dispatch_g1(int NP, const CUtensorMap* m, const G1Params& P, int grid, cudaStream_t s) {
+  switch (NP) {
+#define CASE(v) \
+  case v:       \
+    return launch_g1<v>(m, P, grid, s);
+    CASE(16) CASE(32) CASE(48) CASE(64) CASE(80) CASE(96) CASE(112) CASE(128)
+    CASE(144) CASE(160) CASE(176) CASE(192) CASE(208) CASE(224) CASE(240) CASE(256)
+#undef CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+int df_mixed_prepare(jk_engine* e, int nocc) {
+  DFState& d = e->df;
+  MixedState& m = e->mixed;
+  const int n = e->obs.n_final, naux = d.naux;
+  const int NP = ((nocc + 15) / 16) * 16;
+  if (NP > 256) return set_error(e, JK_ERR_ARG, "mixed DF: nocc above 256 is not supported");
+  const int ldb = ((n + BK - 1) / BK) * BK;
+  cudaStream_t s = e->stream;
+  cudaError_t st = cudaSuccess;
+  if (!m.ready || m.ldb != ldb) {
+    const size_t rows = (size_t)n * naux;
+    st = m.Bh.alloc(rows * ldb);
+    if (st == cudaSuccess) st = m.Bl.alloc(rows * ldb);
+    if (st != cudaSuccess) return check_cuda(e, st, "mixed B allocation");
+    const size_t tot = rows * ldb;
+    k_split_B<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(rows, n, ldb, d.B64.p, m.Bh.p, m.Bl.p);
+    st = cudaGetLastError();
+    if (st != cudaSuccess) return check_cuda(e, st, "split B");
+    m.ldb = ldb;
+    m.NP = 0;
+    m.ready = true;
+  }
+  if (m.NP != NP) {
+    st = m.Ch.alloc((size_t)NP * ldb);
+    if (st == cudaSuccess) st = m.Cl.alloc((size_t)NP * ldb);
+    if (st == cudaSuccess) st = m.Xh.alloc((size_t)n * naux * NP);
+    if (st == cudaSuccess) st = m.Xl.alloc((size_t)n * naux * NP);
+    if (st == cudaSuccess) st = m.Kt.alloc((size_t)n * n);
+    if (st == cudaSuccess) st = m.err.alloc(1);
+    if (st == cudaSuccess) st = d.gamma.alloc(naux);
+    if (st != cudaSuccess) return check_cuda(e, st, "mixed scratch allocation");
+    cudaMemsetAsync(m.err.p, 0, sizeof(int), s);
+    bool ok = make_map(&m.maps[0], m.Bh.p, ldb, (uint64_t)n * naux, BK, BM) &&
+              make_map(&m.maps[1], m.Bl.p, ldb, (uint64_t)n * naux, BK, BM) &&
+              make_map(&m.maps[2], m.Ch.p, ldb, NP, BK, NP) && make_map(&m.maps[3], m.Cl.p, ldb, NP, BK, NP) &&
+              make_map(&m.maps[4], m.Xh.p, (uint64_t)naux * NP, n, BK, BM) &&
+              make_map(&m.maps[5], m.Xl.p, (uint64_t)naux * NP, n, BK, BM);
+    if (!ok) return set_error(e, JK_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    m.NP = NP;
+  }
+  return JK_OK;
+}
+
+int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double* dK, cudaStream_t s) {
+  int rc = df_mixed_prepare(e, nocc);
+  if (rc) return rc;
+  DFState& d = e->df;
+  MixedState& m = e->mixed;
+  const int n = e->obs.n_final, naux = d.naux, NP = m.NP, ldb = m.ldb;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device);
+  stage_mark(e, 0, s);
+  k_split_C<<<dim3((ldb + 127) / 128, NP), 128, 0, s>>>(n, nocc, NP, ldb, dC, m.Ch.p, m.Cl.p);
+  cudaMemsetAsync(d.gamma.p, 0, sizeof(double) * naux, s);
+  cudaMemsetAsync(m.Kt.p, 0, sizeof(float) * n * n, s);
+  cudaMemsetAsync(dJ, 0, sizeof(double) * n * n, s);
+  G1Params P1{};
+  P1.M = n * naux;
+  P1.kblocks = ldb / BK;
+  P1.nocc = nocc;
+  P1.n = n;
+  P1.naux = naux;
+  P1.ntiles = (P1.M + BM - 1) / BM;
+  P1.C = dC;
+  P1.Xhi = m.Xh.p;
+  P1.Xlo = m.Xl.p;
+  P1.gamma = d.gamma.p;
+  P1.err = m.err.p;
+  cudaError_t st = dispatch_g1(NP, m.maps, P1, std::min(nsm, P1.ntiles), s);
+  if (st != cudaSuccess) return check_cuda(e, st, "gemm1 launch");
+  stage_mark(e, 1, s);
+  G2Params P2{};
+  P2.n = n;
+  P2.kblocks = (naux * NP) / BK;
+  P2.ntile_n = (n + BM - 1) / BM;
+  P2.ntiles_u = P2.ntile_n * (P2.ntile_n + 1) / 2;
+  P2.splits = std::max(1, std::min(nsm / P2.ntiles_u, P2.kblocks));
+  P2.Kt = m.Kt.p;
+  P2.err = m.err.p;
+  st = cudaFuncSetAttribute(k_gemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, G2_SMEM);
+  if (st != cudaSuccess) return check_cuda(e, st, "gemm2 attribute");
+  k_gemm2<<<P2.ntiles_u * P2.splits, 192, G2_SMEM, s>>>(m.maps[4], m.maps[5], P2);
+  st = cudaGetLastError();
+  if (st != cudaSuccess) return check_cuda(e, st, "gemm2 launch");
+  stage_mark(e, 2, s);
+  const int kchunk = 64;
+  k_J_mixed<<<dim3(n, (naux + kchunk - 1) / kchunk), (ldb + 7) / 8, 0, s>>>(n, naux, ldb, kchunk, m.Bh.p, m.Bl.p,
+                                                                            d.gamma.p, dJ);
+  stage_mark(e, 3, s);
+  const size_t nn = (size_t)n * n;
+  k_finalize_mixed<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(n, m.Kt.p, dJ, dK);
+  stage_mark(e, 4, s);
+  return check_cuda(e, cudaGetLastError(), "mixed DF launch");
+}
+
+int df_mixed_error(jk_engine* e) {
+  if (!e->mixed.err.p) return JK_OK;
+  int h = 0;
+  cudaError_t st = cudaMemcpyAsync(&h, e->mixed.err.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
+  if (st != cudaSuccess) return check_cuda(e, st, "mixed DF error word");
+  if (h) {
+    cudaMemsetAsync(e->mixed.err.p, 0, sizeof(int), e->stream);
+    return set_error(e, JK_ERR_CUDA, "mixed DF: tensor-core pipeline wait timed out (stage " + std::to_string(h) + ")");
+  }
+  return JK_OK;
+}
+
+}  // namespace m2

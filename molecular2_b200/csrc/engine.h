@@ -1,6 +1,8 @@
 // Internal engine state shared by the .cu translation units (not part of the C ABI).
 #pragma once
 #include <cublas_v2.h>
+#include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
@@ -85,6 +87,19 @@ struct DFState {
   DevBuf<double> gamma;    // naux
 };
 
+// Split-BF16 copies and scratch of the tensor-core (mixed) DF path.
+struct MixedState {
+  bool ready = false;
+  int ldb = 0;                       // padded row length of Bh/Bl (multiple of 64)
+  int NP = 0;                        // nocc padded to a multiple of 16
+  DevBuf<__nv_bfloat16> Bh, Bl;      // [x][K][y], ld = ldb
+  DevBuf<__nv_bfloat16> Ch, Cl;      // [i][y] (NP x ldb)
+  DevBuf<__nv_bfloat16> Xh, Xl;      // [x][K][i] (n x naux*NP)
+  DevBuf<float> Kt;                  // n x n partial K (lower-triangle tiles)
+  DevBuf<int> err;                   // pipeline error word
+  CUtensorMap maps[6];               // Bh, Bl, Ch, Cl, Xh, Xl
+};
+
 }  // namespace m2
 
 struct jk_engine {
@@ -117,6 +132,7 @@ struct jk_engine {
   // scratch for J/K builds
   m2::DevBuf<double> Dcart, Jcart, Kcart, Dnorm, Dmax, Dfinal, Jfinal, Kfinal;
   m2::DFState df;
+  m2::MixedState mixed;
   long long last_quartets = 0;
   // optional per-stage CUDA-event timing of the DF build (jk_set_profiling)
   bool profiling = false;
@@ -139,6 +155,10 @@ int direct_jk_device(jk_engine* e, const double* dD, double precision, double mu
 int df_setup(jk_engine* e);
 int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ, double* dK, cudaStream_t s);
 int one_body_device(jk_engine* e, double* S, double* T, double* V, cudaStream_t s);
+void stage_mark(jk_engine* e, int k, cudaStream_t s);
+// df_mixed.cu
+int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double* dK, cudaStream_t s);
+int df_mixed_error(jk_engine* e);
 // transforms (cart <-> final) and norms
 void launch_final_to_cart(const jk_engine* e, const double* Dfinal, double* Dcart, cudaStream_t s);
 void launch_cart_to_final_sym(const jk_engine* e, const double* Xcart, double scale, double* Xfinal, cudaStream_t s);

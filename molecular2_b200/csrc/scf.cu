@@ -231,7 +231,10 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     cudaStreamSynchronize(s);
   }
   double jk_ms = 0.0;
-  int builds = 0;
+  int builds = 0, mixed_builds = 0, fp64_after_switch = 0;
+  const bool mixed = o->df && o->prec_mode == 1;
+  const double mixed_switch = o->mixed_switch > 0.0 ? o->mixed_switch : 1e-5;
+  bool switched = !mixed;  // mixed-precision builds until the density settles
   const double enuc = o->enuc;
   // state of Fock (src/fock.cpp:32-74)
   bool started_incremental = false, reset_incremental = false, have_dens = false;
@@ -270,7 +273,12 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     cudaEventRecord(a, s);
     int rc2;
     if (o->df) {
-      rc2 = df_jk_device(e, C.p, nocc, o->prec_mode, J.p, K.p, s);
+      const int mode = switched ? 0 : 1;
+      rc2 = df_jk_device(e, C.p, nocc, mode, J.p, K.p, s);
+      if (mode == 1)
+        ++mixed_builds;
+      else if (mixed)
+        ++fp64_after_switch;
       if (!rc2) {
         g.copy(J.p, G, nn);
         g.scal(2.0, G, nn);
@@ -385,6 +393,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     g.copy(D.p, t1.p, nn);
     g.axpy(-1.0, Dold.p, t1.p, nn);
     dd = g.nrm2(t1.p, nn);
+    if (!switched && dd < mixed_switch) switched = true;
     g.copy(D.p, Dold.p, nn);
     if ((rc = make_fock())) return cleanup(), rc;
     calc_err();
@@ -395,8 +404,13 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     delta = std::fabs(energy - last_energy);
     if (it > 2) average(weights);
     transform(F.p);
-    converged = dd < o->densconverge && delta < o->enconverge;
+    // a mixed run only converges on energies of two FP64 builds
+    converged = dd < o->densconverge && delta < o->enconverge && (!mixed || fp64_after_switch >= 2);
     ++it;
+  }
+  if (mixed) {
+    int rc2 = df_mixed_error(e);
+    if (rc2) return cleanup(), rc2;
   }
   if (!diagonalise()) return cleanup(), set_error(e, JK_ERR_CUDA, "syevd(F)");
   st = cudaStreamSynchronize(s);
@@ -409,6 +423,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   r->jk_ms = jk_ms;
   r->last_delta_e = delta;
   r->last_delta_d = dd;
+  r->mixed_builds = mixed_builds;
   if (o->out_density) cudaMemcpy(o->out_density, D.p, nn * sizeof(double), cudaMemcpyDeviceToHost);
   if (o->out_coeffs) cudaMemcpy(o->out_coeffs, C.p, nn * sizeof(double), cudaMemcpyDeviceToHost);
   if (o->out_eps) cudaMemcpy(o->out_eps, eps.p, n * sizeof(double), cudaMemcpyDeviceToHost);
