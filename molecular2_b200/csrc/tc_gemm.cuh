@@ -13,7 +13,7 @@ namespace tc {
 
 // Every wait gives up after this many polls and reports the failure; a
 // correct schedule never comes near it (each poll may also suspend briefly).
-constexpr uint32_t WAIT_LIMIT = 1u << 26;
+constexpr uint32_t WAIT_LIMIT = 1u << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
