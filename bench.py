@@ -156,7 +156,7 @@ class Clocks:
 
 
 def roofline_fp64(n, naux, nocc, stages):
-    names = ["X=B.C (cuBLAS DGEMM)", "K=X.X^T (cuBLAS DSYRK)", "gamma (k_gamma)", "J=B.gamma (k_df_J)"]
+    names = ["X=B.C (cuBLAS DGEMM)", "K=X.X^T (cuBLAS DGEMM)", "gamma (k_gamma)", "J=B.gamma (k_df_J)"]
     hbm, bf16, src = peaks()
     B_bytes = n * n * naux * 8
     own = 3

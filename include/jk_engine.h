@@ -126,8 +126,12 @@ typedef struct jk_scf_options {
   int nocc;
   int df;                  /* 0 = integral-direct J/K, 1 = density-fitted */
   int prec_mode;           /* DF only: 0 = FP64; 1 = split-BF16 tensor-core builds while
-                              ||D - D_old||_F >= mixed_switch, FP64 builds after that */
-  double mixed_switch;     /* default 1e-5 */
+                              ||D - D_old||_F >= mixed_switch, then mixed builds plus an
+                              FP64 correction G64 - Gmixed taken at the switch density,
+                              and the energy from a final FP64 build */
+  double mixed_switch;     /* default 1e-3 */
+  int eig_mode;            /* 0 = cuSOLVER syevd every iteration; 1 = Jacobi (syevj) on the
+                              Fock matrix in the previous eigenvectors after the first */
   int maxiter;             /* molecular2 default 40 */
   int maxdiis;             /* default 8 */
   int diis;                /* 1 = on */
@@ -151,6 +155,7 @@ typedef struct jk_scf_result {
   double last_delta_e;
   double last_delta_d;
   int mixed_builds;        /* J/K builds done in mixed precision */
+  double diag_ms;          /* device time in the Fock diagonalisations */
 } jk_scf_result;
 
 int jk_scf_rhf(jk_engine* e, const jk_scf_options* opt, jk_scf_result* res);

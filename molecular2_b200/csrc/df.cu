@@ -155,13 +155,6 @@ __global__ void k_lower_only(int n, double* A) {  // zero the strict upper trian
   if (i < (size_t)n * n && (int)(i % n) < (int)(i / n)) A[i] = 0.0;
 }
 
-__global__ void k_sym_from_lower(int n, double* A) {  // A[j][i] = A[i][j] for i > j (col-major lower)
-  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= (size_t)n * n) return;
-  const int r = (int)(k % n), c = (int)(k / n);
-  if (r < c) A[k] = A[(size_t)r * n + c];
-}
-
 // gamma_K = sum_{x,i} X[x][K][i] C[x][i]   (C column-major n x o)
 __global__ void k_gamma(int n, int naux, int o, const double* __restrict__ X, const double* __restrict__ C,
                         double* __restrict__ g) {
@@ -273,12 +266,11 @@ int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ,
                   nocc) != CUBLAS_STATUS_SUCCESS)
     return set_error(e, JK_ERR_CUDA, "X = B C gemm");
   stage_mark(e, 1, s);
-  // K = X^T X over the (naux*o) inner index
-  if (cublasDsyrk(e->cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, naux * nocc, &one, d.X64.p, naux * nocc, &zero,
-                  dK, n) != CUBLAS_STATUS_SUCCESS)
-    return set_error(e, JK_ERR_CUDA, "K = X X^T syrk");
-  const int nb = 256;
-  k_sym_from_lower<<<(unsigned)(((size_t)n * n + nb - 1) / nb), nb, 0, s>>>(n, dK);
+  // K = X^T X over the (naux*o) inner index (a full DGEMM: on this part
+  // cuBLAS DGEMM outruns DSYRK although it does twice the flops)
+  if (cublasDgemm(e->cublas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, naux * nocc, &one, d.X64.p, naux * nocc, d.X64.p,
+                  naux * nocc, &zero, dK, n) != CUBLAS_STATUS_SUCCESS)
+    return set_error(e, JK_ERR_CUDA, "K = X^T X gemm");
   stage_mark(e, 2, s);
   k_gamma<<<naux, 256, 0, s>>>(n, naux, nocc, d.X64.p, dC, d.gamma.p);
   stage_mark(e, 3, s);

@@ -192,10 +192,10 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   cudaStream_t s = e->stream;
   cublasSetStream(e->cublas, s);
   Gpu g{e, s, n};
-  DevBuf<double> S, T, V, H, X, F, Fm, Finc, D, Dd, Dold, C, W, eps, J, K, t1, t2, err, work;
+  DevBuf<double> S, T, V, H, X, F, Fm, Finc, D, Dd, Dold, C, W, Wt, eps, J, K, t1, t2, err, work, Delta;
   DevBuf<int> info;
   cudaError_t st = cudaSuccess;
-  for (auto* b : {&S, &T, &V, &H, &X, &F, &Fm, &Finc, &D, &Dd, &Dold, &C, &W, &J, &K, &t1, &t2, &err})
+  for (auto* b : {&S, &T, &V, &H, &X, &F, &Fm, &Finc, &D, &Dd, &Dold, &C, &W, &Wt, &J, &K, &t1, &t2, &err, &Delta})
     if (st == cudaSuccess) st = b->alloc(nn);
   if (st == cudaSuccess) st = eps.alloc(n);
   if (st == cudaSuccess) st = info.alloc(1);
@@ -204,14 +204,33 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   if (rc) return rc;
   g.copy(T.p, H.p, nn);
   g.axpy(1.0, V.p, H.p, nn);
-  // syevd workspace
-  int lwork = 0;
+  // eigensolvers: divide and conquer (syevd), and Jacobi (syevj) warm-started
+  // on the Fock matrix expressed in the previous eigenvectors, which is nearly
+  // diagonal once the SCF settles (eig_mode 1)
+  int lwork = 0, lwork_j = 0;
+  syevjInfo_t jinfo = nullptr;
+  cusolverDnCreateSyevjInfo(&jinfo);
+  cusolverDnXsyevjSetTolerance(jinfo, 1e-14);
+  cusolverDnXsyevjSetMaxSweeps(jinfo, 50);
   cusolverDnDsyevd_bufferSize(e->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, W.p, n, eps.p, &lwork);
-  if ((st = work.alloc(std::max(lwork, 1))) != cudaSuccess) return check_cuda(e, st, "syevd workspace");
+  cusolverDnDsyevj_bufferSize(e->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, W.p, n, eps.p,
+                              &lwork_j, jinfo);
+  struct JinfoGuard {
+    syevjInfo_t p;
+    ~JinfoGuard() {
+      if (p) cusolverDnDestroySyevjInfo(p);
+    }
+  } jguard{jinfo};
+  if ((st = work.alloc(std::max(std::max(lwork, lwork_j), 1))) != cudaSuccess)
+    return check_cuda(e, st, "eigensolver workspace");
   auto syev = [&](const double* A, double* vecs, double* vals) -> bool {
     g.copy(A, vecs, nn);
     return cusolverDnDsyevd(e->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, vecs, n, vals, work.p,
                             lwork, info.p) == CUSOLVER_STATUS_SUCCESS;
+  };
+  auto syevj_inplace = [&](double* A, double* vals) -> bool {
+    return cusolverDnDsyevj(e->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n, vals, work.p,
+                            lwork_j, info.p, jinfo) == CUSOLVER_STATUS_SUCCESS;
   };
   // S^-1/2 = U lambda^-1/2 U^T (Fock::formOrthog, src/fock.cpp:124-142)
   std::vector<double> lam(n);
@@ -230,11 +249,26 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     g.mm(false, true, t1.p, W.p, X.p);                                              // (U diag) U^T
     cudaStreamSynchronize(s);
   }
-  double jk_ms = 0.0;
-  int builds = 0, mixed_builds = 0, fp64_after_switch = 0;
+  double jk_ms = 0.0, diag_ms = 0.0;
+  int builds = 0, mixed_builds = 0, corrected_builds = 0;
+  // Mixed precision (DF only): split-BF16 builds while ||dD|| >= mixed_switch;
+  // then one FP64 build and one mixed build at the same density give the
+  // precision correction Delta = G64 - Gmixed, and later iterations use
+  // Gmixed(D) + Delta (error ~ eps |D - D_switch| instead of eps |D|); the
+  // reported energy comes from a final FP64 build at the converged density.
   const bool mixed = o->df && o->prec_mode == 1;
-  const double mixed_switch = o->mixed_switch > 0.0 ? o->mixed_switch : 1e-5;
-  bool switched = !mixed;  // mixed-precision builds until the density settles
+  const double mixed_switch = o->mixed_switch > 0.0 ? o->mixed_switch : 1e-3;
+  bool switched = !mixed, have_delta = false;
+  cudaEvent_t ev_a, ev_b;
+  cudaEventCreate(&ev_a);
+  cudaEventCreate(&ev_b);
+  struct EvGuard {
+    cudaEvent_t a, b;
+    ~EvGuard() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } evguard{ev_a, ev_b};
   const double enuc = o->enuc;
   // state of Fock (src/fock.cpp:32-74)
   bool started_incremental = false, reset_incremental = false, have_dens = false;
@@ -250,9 +284,29 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     g.mm(false, false, Fa, X.p, t1.p);
     g.mm(true, false, X.p, t1.p, Fm.p);
   };
+  bool have_W = false;  // W holds the eigenvectors of the previous Fm
   auto diagonalise = [&]() -> bool {
-    if (!syev(Fm.p, W.p, eps.p)) return false;
-    return g.mm(false, false, X.p, W.p, C.p);
+    cudaEventRecord(ev_a, s);
+    bool ok;
+    if (o->eig_mode == 1 && have_W) {
+      g.mm(false, false, Fm.p, W.p, t1.p);
+      g.mm(true, false, W.p, t1.p, Wt.p);  // W^T Fm W
+      ok = syevj_inplace(Wt.p, eps.p);
+      if (ok) {
+        g.mm(false, false, W.p, Wt.p, t1.p);
+        g.copy(t1.p, W.p, nn);
+      }
+    } else {
+      ok = syev(Fm.p, W.p, eps.p);
+    }
+    have_W = ok;
+    ok = ok && g.mm(false, false, X.p, W.p, C.p);
+    cudaEventRecord(ev_b, s);
+    cudaEventSynchronize(ev_b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev_a, ev_b);
+    diag_ms += ms;
+    return ok;
   };
   auto make_dens = [&]() {
     if (have_dens) {
@@ -266,19 +320,16 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
       g.axpy(1.0, D.p, Dd.p, nn);
     have_dens = true;
   };
-  auto jk = [&](const double* P, double* G) -> int {  // G = J - 1/2 K (direct) or 2J - K (DF, w.r.t. C)
+  // G = J - 1/2 K (direct, w.r.t. P) or 2J - K (DF, w.r.t. the occupied C)
+  auto jk = [&](const double* P, double* G, int mode) -> int {
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     cudaEventRecord(a, s);
     int rc2;
     if (o->df) {
-      const int mode = switched ? 0 : 1;
       rc2 = df_jk_device(e, C.p, nocc, mode, J.p, K.p, s);
-      if (mode == 1)
-        ++mixed_builds;
-      else if (mixed)
-        ++fp64_after_switch;
+      if (mode == 1) ++mixed_builds;
       if (!rc2) {
         g.copy(J.p, G, nn);
         g.scal(2.0, G, nn);
@@ -319,12 +370,27 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
         last_reset = fock_iter;
         next_reset = rms_error / 1e1;
       }
-      int rc2 = jk(Dd.p, t2.p);
+      int rc2 = jk(Dd.p, t2.p, 0);
       if (rc2) return rc2;
       g.axpy(1.0, t2.p, F.p, nn);
       g.copy(F.p, Finc.p, nn);
     } else {
-      int rc2 = jk(nullptr, t2.p);
+      int rc2 = JK_OK;
+      if (!switched) {
+        rc2 = jk(nullptr, t2.p, 1);
+      } else if (mixed && !have_delta) {
+        if ((rc2 = jk(nullptr, Delta.p, 1))) return rc2;
+        if ((rc2 = jk(nullptr, t2.p, 0))) return rc2;
+        g.scal(-1.0, Delta.p, nn);
+        g.axpy(1.0, t2.p, Delta.p, nn);  // Delta = G64 - Gmixed
+        have_delta = true;
+      } else if (mixed) {
+        if ((rc2 = jk(nullptr, t2.p, 1))) return rc2;
+        g.axpy(1.0, Delta.p, t2.p, nn);
+        ++corrected_builds;
+      } else {
+        rc2 = jk(nullptr, t2.p, 0);
+      }
       if (rc2) return rc2;
       g.copy(H.p, F.p, nn);
       g.axpy(1.0, t2.p, F.p, nn);
@@ -393,7 +459,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     g.copy(D.p, t1.p, nn);
     g.axpy(-1.0, Dold.p, t1.p, nn);
     dd = g.nrm2(t1.p, nn);
-    if (!switched && dd < mixed_switch) switched = true;
+    if (!switched && dd < mixed_switch) switched = true;  // takes effect in this iteration's build
     g.copy(D.p, Dold.p, nn);
     if ((rc = make_fock())) return cleanup(), rc;
     calc_err();
@@ -404,13 +470,18 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     delta = std::fabs(energy - last_energy);
     if (it > 2) average(weights);
     transform(F.p);
-    // a mixed run only converges on energies of two FP64 builds
-    converged = dd < o->densconverge && delta < o->enconverge && (!mixed || fp64_after_switch >= 2);
+    // a mixed run only converges on corrected builds
+    converged = dd < o->densconverge && delta < o->enconverge && (!mixed || corrected_builds >= 2);
     ++it;
   }
   if (mixed) {
     int rc2 = df_mixed_error(e);
     if (rc2) return cleanup(), rc2;
+    // energy of the converged density with an FP64 Fock build
+    if ((rc2 = jk(nullptr, t2.p, 0))) return cleanup(), rc2;
+    g.copy(H.p, F.p, nn);
+    g.axpy(1.0, t2.p, F.p, nn);
+    calc_e();
   }
   if (!diagonalise()) return cleanup(), set_error(e, JK_ERR_CUDA, "syevd(F)");
   st = cudaStreamSynchronize(s);
@@ -424,6 +495,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   r->last_delta_e = delta;
   r->last_delta_d = dd;
   r->mixed_builds = mixed_builds;
+  r->diag_ms = diag_ms;
   if (o->out_density) cudaMemcpy(o->out_density, D.p, nn * sizeof(double), cudaMemcpyDeviceToHost);
   if (o->out_coeffs) cudaMemcpy(o->out_coeffs, C.p, nn * sizeof(double), cudaMemcpyDeviceToHost);
   if (o->out_eps) cudaMemcpy(o->out_eps, eps.p, n * sizeof(double), cudaMemcpyDeviceToHost);
