@@ -129,7 +129,8 @@ typedef struct jk_scf_options {
                               ||D - D_old||_F >= mixed_switch, then mixed builds plus an
                               FP64 correction G64 - Gmixed taken at the switch density,
                               and the energy from a final FP64 build */
-  double mixed_switch;     /* default 1e-3 */
+  double mixed_switch;     /* default 1e-3; the switch also happens when ||dD|| stalls */
+  int mixed_refresh;       /* iterations between FP64 refreshes of the correction, default 4 */
   int eig_mode;            /* 0 = cuSOLVER syevd every iteration; 1 = Jacobi (syevj) on the
                               Fock matrix in the previous eigenvectors after the first */
   int maxiter;             /* molecular2 default 40 */

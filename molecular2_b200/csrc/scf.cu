@@ -12,6 +12,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -103,15 +104,42 @@ void full_piv_solve(std::vector<double> A, int N, std::vector<double> b, std::ve
   for (int i = 0; i < N; ++i) x[cp[i]] = y[i];
 }
 
+// FIFO of at most `cap` device vectors backed by buffers allocated once, so
+// the SCF loop never allocates (cudaFree would synchronise the device).
+struct Ring {
+  std::vector<std::unique_ptr<DevBuf<double>>> pool;
+  std::vector<double*> order;  // oldest first
+  std::vector<double*> spare;
+  cudaError_t init(int cap, size_t len) {
+    for (int i = 0; i < cap + 1; ++i) {
+      pool.emplace_back(new DevBuf<double>());
+      cudaError_t st = pool.back()->alloc(len);
+      if (st != cudaSuccess) return st;
+      spare.push_back(pool.back()->p);
+    }
+    return cudaSuccess;
+  }
+  void pop_front() {
+    spare.push_back(order.front());
+    order.erase(order.begin());
+  }
+  double* push() {
+    if (spare.empty()) pop_front();
+    double* p = spare.back();
+    spare.pop_back();
+    order.push_back(p);
+    return p;
+  }
+  size_t size() const { return order.size(); }
+  double* operator[](size_t i) const { return order[i]; }
+};
+
 struct Diis {  // DIISEngine (src/diis.cpp) with error vectors in HBM
   int max = 8;
   bool use = true;
-  std::vector<DevBuf<double>*> errs;
+  Ring errs;
   std::vector<double> lastB{0.0};
   int lastB_dim = 1;
-  ~Diis() {
-    for (auto* p : errs) delete p;
-  }
 
   static std::vector<double> solve(const std::vector<double>& B, int dim, int start) {
     const int size = dim - start;
@@ -136,16 +164,11 @@ struct Diis {  // DIISEngine (src/diis.cpp) with error vectors in HBM
     std::vector<double> weights;
     const int it = (int)errs.size() + 1;
     if (!use) return weights;
-    if (it > max) {
-      delete errs.front();
-      errs.erase(errs.begin());
-    }
-    auto* nb = new DevBuf<double>();
-    nb->alloc(len);
-    g.copy(err, nb->p, len);
-    errs.push_back(nb);
+    if (it > max) errs.pop_front();
+    double* nb = errs.push();
+    g.copy(err, nb, len);
     if (it == 1) {
-      lastB.assign(1, g.dot(nb->p, nb->p, len));
+      lastB.assign(1, g.dot(nb, nb, len));
       lastB_dim = 1;
     }
     if (it > 1) {
@@ -158,7 +181,7 @@ struct Diis {  // DIISEngine (src/diis.cpp) with error vectors in HBM
         B[(size_t)lim * dim + i] = B[(size_t)i * dim + lim] = -1.0;
       }
       for (int i = 0; i < lim; ++i) {
-        double v = g.dot(errs[i]->p, errs[lim - 1]->p, len);
+        double v = g.dot(errs[i], errs[lim - 1], len);
         B[(size_t)(lim - 1) * dim + i] = B[(size_t)i * dim + lim - 1] = v;
       }
       B[(size_t)lim * dim + lim - 1] = B[(size_t)(lim - 1) * dim + lim] = -1.0;
@@ -251,14 +274,19 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   }
   double jk_ms = 0.0, diag_ms = 0.0;
   int builds = 0, mixed_builds = 0, corrected_builds = 0;
-  // Mixed precision (DF only): split-BF16 builds while ||dD|| >= mixed_switch;
-  // then one FP64 build and one mixed build at the same density give the
-  // precision correction Delta = G64 - Gmixed, and later iterations use
-  // Gmixed(D) + Delta (error ~ eps |D - D_switch| instead of eps |D|); the
-  // reported energy comes from a final FP64 build at the converged density.
+  // Mixed precision (DF only): split-BF16 builds until ||dD|| < mixed_switch
+  // or the density change stalls (no halving over three iterations: the floor
+  // set by the mixed builds' own error).  From then on one FP64 build and one
+  // mixed build at the same density give the correction Delta = G64 - Gmixed,
+  // refreshed every mixed_refresh iterations, and the other iterations use
+  // Gmixed(D) + Delta, whose error scales with |D - D_refresh| instead of |D|.
+  // The reported energy comes from a final FP64 build at the converged density.
   const bool mixed = o->df && o->prec_mode == 1;
   const double mixed_switch = o->mixed_switch > 0.0 ? o->mixed_switch : 1e-3;
+  const int refresh_every = o->mixed_refresh > 0 ? o->mixed_refresh : 4;
   bool switched = !mixed, have_delta = false;
+  int since_refresh = 0, refreshes = 0;
+  double dd_hist[3] = {1e300, 1e300, 1e300};
   cudaEvent_t ev_a, ev_b;
   cudaEventCreate(&ev_a);
   cudaEventCreate(&ev_b);
@@ -276,10 +304,12 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   const double incremental_threshold = 1e-5;
   int last_reset = 0, fock_iter = 0;
   const int MAX = o->maxdiis > 0 ? o->maxdiis : 8;
-  std::vector<DevBuf<double>*> focks;
+  Ring focks;
   Diis diis;
   diis.max = MAX;
   diis.use = o->diis != 0;
+  if ((st = focks.init(MAX, nn)) != cudaSuccess || (st = diis.errs.init(MAX, nn)) != cudaSuccess)
+    return check_cuda(e, st, "scf DIIS history");
   auto transform = [&](const double* Fa) {  // Fm = X^T F X
     g.mm(false, false, Fa, X.p, t1.p);
     g.mm(true, false, X.p, t1.p, Fm.p);
@@ -378,16 +408,19 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
       int rc2 = JK_OK;
       if (!switched) {
         rc2 = jk(nullptr, t2.p, 1);
-      } else if (mixed && !have_delta) {
+      } else if (mixed && (!have_delta || since_refresh >= refresh_every)) {
         if ((rc2 = jk(nullptr, Delta.p, 1))) return rc2;
         if ((rc2 = jk(nullptr, t2.p, 0))) return rc2;
         g.scal(-1.0, Delta.p, nn);
         g.axpy(1.0, t2.p, Delta.p, nn);  // Delta = G64 - Gmixed
         have_delta = true;
+        since_refresh = 0;
+        ++refreshes;
       } else if (mixed) {
         if ((rc2 = jk(nullptr, t2.p, 1))) return rc2;
         g.axpy(1.0, Delta.p, t2.p, nn);
         ++corrected_builds;
+        ++since_refresh;
       } else {
         rc2 = jk(nullptr, t2.p, 0);
       }
@@ -396,14 +429,8 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
       g.axpy(1.0, t2.p, F.p, nn);
     }
     if (o->diis) {
-      if (fock_iter >= MAX) {
-        delete focks.front();
-        focks.erase(focks.begin());
-      }
-      auto* f = new DevBuf<double>();
-      f->alloc(nn);
-      g.copy(F.p, f->p, nn);
-      focks.push_back(f);
+      if (fock_iter >= MAX) focks.pop_front();
+      g.copy(F.p, focks.push(), nn);
       ++fock_iter;
     }
     return JK_OK;
@@ -427,12 +454,10 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     if (o->diis && fock_iter > 2) {
       const int off = (int)focks.size() - (int)w.size();
       cudaMemsetAsync(F.p, 0, nn * sizeof(double), s);
-      for (int i = off; i < (int)focks.size(); ++i) g.axpy(w[i - off], focks[i]->p, F.p, nn);
+      for (int i = off; i < (int)focks.size(); ++i) g.axpy(w[i - off], focks[i], F.p, nn);
     }
   };
-  auto cleanup = [&]() {
-    for (auto* f : focks) delete f;
-  };
+  auto cleanup = [&]() {};
   // guess (Fock::transform(true)): core Hamiltonian, or a caller-supplied AO Fock
   if (o->guess_fock) {
     cudaMemcpyAsync(F.p, o->guess_fock, nn * sizeof(double), cudaMemcpyHostToDevice, s);
@@ -459,7 +484,11 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     g.copy(D.p, t1.p, nn);
     g.axpy(-1.0, Dold.p, t1.p, nn);
     dd = g.nrm2(t1.p, nn);
-    if (!switched && dd < mixed_switch) switched = true;  // takes effect in this iteration's build
+    if (!switched) {  // takes effect in this iteration's build
+      const double best = std::min(dd_hist[0], std::min(dd_hist[1], dd_hist[2]));
+      if (dd < mixed_switch || (it >= 6 && dd > 0.5 * best)) switched = true;
+      dd_hist[it % 3] = dd;
+    }
     g.copy(D.p, Dold.p, nn);
     if ((rc = make_fock())) return cleanup(), rc;
     calc_err();
@@ -470,8 +499,8 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     delta = std::fabs(energy - last_energy);
     if (it > 2) average(weights);
     transform(F.p);
-    // a mixed run only converges on corrected builds
-    converged = dd < o->densconverge && delta < o->enconverge && (!mixed || corrected_builds >= 2);
+    // a mixed run only converges once its builds carry the FP64 correction
+    converged = dd < o->densconverge && delta < o->enconverge && (!mixed || (have_delta && refreshes >= 2));
     ++it;
   }
   if (mixed) {

@@ -51,7 +51,8 @@ SIGNATURES = {
 
 class SCFOptions(ctypes.Structure):
     """ctypes image of ``jk_scf_options``; defaults are molecular2's (src/ProgramController.cpp:296-307)."""
-    _fields_ = [("nocc", _I), ("df", _I), ("prec_mode", _I), ("mixed_switch", _D), ("eig_mode", _I),
+    _fields_ = [("nocc", _I), ("df", _I), ("prec_mode", _I), ("mixed_switch", _D), ("mixed_refresh", _I),
+                ("eig_mode", _I),
                 ("maxiter", _I), ("maxdiis", _I), ("diis", _I),
                 ("precision", _D), ("enconverge", _D), ("densconverge", _D), ("enuc", _D),
                 ("guess_fock", _P), ("out_density", _P), ("out_coeffs", _P), ("out_eps", _P)]
@@ -201,12 +202,13 @@ class IntegralEngine:
         return S, T, V
 
     def scf_rhf(self, nocc, enuc, df=False, prec_mode=0, maxiter=40, maxdiis=8, diis=True, precision=1e-12,
-                enconverge=1e-7, densconverge=1e-4, guess_fock=None, want=False, mixed_switch=1e-3, eig_mode=0):
+                enconverge=1e-7, densconverge=1e-4, guess_fock=None, want=False, mixed_switch=1e-3, eig_mode=0,
+                mixed_refresh=4):
         """SCF::rhf on the device; returns (SCFResult, extras dict)."""
         n = self.n
         o = SCFOptions()
         o.nocc, o.df, o.prec_mode, o.maxiter, o.maxdiis, o.diis = nocc, int(df), prec_mode, maxiter, maxdiis, int(diis)
-        o.mixed_switch, o.eig_mode = mixed_switch, eig_mode
+        o.mixed_switch, o.eig_mode, o.mixed_refresh = mixed_switch, eig_mode, mixed_refresh
         o.precision, o.enconverge, o.densconverge, o.enuc = precision, enconverge, densconverge, enuc
         keep = []
         if guess_fock is not None:
