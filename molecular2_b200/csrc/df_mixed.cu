@@ -222,7 +222,8 @@ struct G2Params {
   int ntile_n;      // ceil(n/128)
   int ntiles_u;     // lower-triangle tiles
   int splits;
-  float* Kt;        // n x n, Kt[y*n + x] = K[x][y] for tile(x) >= tile(y)
+  double* Kt;       // n x n, Kt[y*n + x] = K[x][y] for tile(x) >= tile(y); FP64 so
+                    // the split-K sum does not depend on the atomics' order
   int* err;
 };
 
@@ -341,7 +342,7 @@ __global__ void __launch_bounds__(192, 1)
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
             const int y = ty * BM + c * 16 + e;
-            if (y < P.n) atomicAdd(P.Kt + (size_t)y * P.n + x, v[e]);
+            if (y < P.n) atomicAdd(P.Kt + (size_t)y * P.n + x, (double)v[e]);
           }
         }
       }
@@ -407,12 +408,12 @@ __global__ void k_J_mixed(int n, int naux, int ldb, int kchunk, const __nv_bfloa
 }
 
 // J: mirror the lower triangle; K: assemble from the lower-triangle tiles of Kt
-__global__ void k_finalize_mixed(int n, const float* __restrict__ Kt, double* __restrict__ J, double* __restrict__ K) {
+__global__ void k_finalize_mixed(int n, const double* __restrict__ Kt, double* __restrict__ J, double* __restrict__ K) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (size_t)n * n) return;
   const int i = (int)(idx % n), j = (int)(idx / n);  // element (i, j), column-major
   const int ti = i / BM, tj = j / BM;
-  K[idx] = (ti >= tj) ? (double)Kt[(size_t)j * n + i] : (double)Kt[(size_t)i * n + j];
+  K[idx] = (ti >= tj) ? Kt[(size_t)j * n + i] : Kt[(size_t)i * n + j];
   if (i < j) J[idx] = J[(size_t)i * n + j];
 }
 __global__ void k_zero_upper(int n, double* J) {
@@ -524,7 +525,7 @@ int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double
   stage_mark(e, 0, s);
   k_split_C<<<dim3((ldb + 127) / 128, NP), 128, 0, s>>>(n, nocc, NP, ldb, dC, m.Ch.p, m.Cl.p);
   cudaMemsetAsync(d.gamma.p, 0, sizeof(double) * naux, s);
-  cudaMemsetAsync(m.Kt.p, 0, sizeof(float) * n * n, s);
+  cudaMemsetAsync(m.Kt.p, 0, sizeof(double) * n * n, s);
   cudaMemsetAsync(dJ, 0, sizeof(double) * n * n, s);
   G1Params P1{};
   P1.M = n * naux;

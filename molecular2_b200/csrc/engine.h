@@ -95,7 +95,7 @@ struct MixedState {
   DevBuf<__nv_bfloat16> Bh, Bl;      // [x][K][y], ld = ldb
   DevBuf<__nv_bfloat16> Ch, Cl;      // [i][y] (NP x ldb)
   DevBuf<__nv_bfloat16> Xh, Xl;      // [x][K][i] (n x naux*NP)
-  DevBuf<float> Kt;                  // n x n partial K (lower-triangle tiles)
+  DevBuf<double> Kt;                 // n x n partial K (lower-triangle tiles)
   DevBuf<int> err;                   // pipeline error word
   CUtensorMap maps[6];               // Bh, Bl, Ch, Cl, Xh, Xl
 };
