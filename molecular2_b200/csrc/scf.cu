@@ -216,9 +216,11 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   cublasSetStream(e->cublas, s);
   Gpu g{e, s, n};
   DevBuf<double> S, T, V, H, X, F, Fm, Finc, D, Dd, Dold, C, W, Wt, eps, J, K, t1, t2, err, work, Delta;
+  DevBuf<double> Cal, Cprev, Um, Vm, Wm;  // orbital alignment of the mixed phase
   DevBuf<int> info;
   cudaError_t st = cudaSuccess;
-  for (auto* b : {&S, &T, &V, &H, &X, &F, &Fm, &Finc, &D, &Dd, &Dold, &C, &W, &Wt, &J, &K, &t1, &t2, &err, &Delta})
+  for (auto* b : {&S, &T, &V, &H, &X, &F, &Fm, &Finc, &D, &Dd, &Dold, &C, &W, &Wt, &J, &K, &t1, &t2, &err, &Delta,
+                  &Cal, &Cprev, &Um, &Vm, &Wm})
     if (st == cudaSuccess) st = b->alloc(nn);
   if (st == cudaSuccess) st = eps.alloc(n);
   if (st == cudaSuccess) st = info.alloc(1);
@@ -350,6 +352,43 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
       g.axpy(1.0, D.p, Dd.p, nn);
     have_dens = true;
   };
+  // Occupied orbitals for the DF build.  In the corrected mixed phase they are
+  // rotated to the set closest to the previous build's (polar factor U of
+  // Cocc^T S Cprev, by Newton-Schulz iterations U <- 1.5 U - 0.5 U U^T U):
+  // J and K depend only on Cocc Cocc^T, so they are unchanged, while the
+  // split-BF16 rounding, which depends on the coefficients themselves, now
+  // changes only as much as the density does.
+  const double* Cuse = C.p;
+  bool have_prev = false;
+  std::vector<double> hU((size_t)nocc * nocc);
+  auto align = [&]() {
+    Cuse = C.p;
+    const size_t no = (size_t)n * nocc, oo = (size_t)nocc * nocc;
+    if (!have_prev) {
+      g.copy(C.p, Cprev.p, no);
+      have_prev = true;
+      return;
+    }
+    g.gemm(false, false, n, nocc, n, 1.0, S.p, n, Cprev.p, n, 0.0, t1.p, n);
+    g.gemm(true, false, nocc, nocc, n, 1.0, C.p, n, t1.p, n, 0.0, Um.p, nocc);
+    for (int k = 0; k < 12; ++k) {
+      g.gemm(true, false, nocc, nocc, nocc, 1.0, Um.p, nocc, Um.p, nocc, 0.0, Wm.p, nocc);
+      g.copy(Um.p, Vm.p, oo);
+      g.gemm(false, false, nocc, nocc, nocc, -0.5, Um.p, nocc, Wm.p, nocc, 1.5, Vm.p, nocc);
+      std::swap(Um.p, Vm.p);
+    }
+    g.gemm(true, false, nocc, nocc, nocc, 1.0, Um.p, nocc, Um.p, nocc, 0.0, Wm.p, nocc);
+    cudaMemcpyAsync(hU.data(), Wm.p, oo * sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    double dev = 0.0;
+    for (int i = 0; i < nocc; ++i)
+      for (int j = 0; j < nocc; ++j) dev = std::max(dev, std::fabs(hU[(size_t)j * nocc + i] - (i == j ? 1.0 : 0.0)));
+    if (dev < 1e-12) {  // a rotation: use it
+      g.gemm(false, false, n, nocc, nocc, 1.0, C.p, n, Um.p, nocc, 0.0, Cal.p, n);
+      Cuse = Cal.p;
+    }
+    g.copy(Cuse, Cprev.p, no);
+  };
   // G = J - 1/2 K (direct, w.r.t. P) or 2J - K (DF, w.r.t. the occupied C)
   auto jk = [&](const double* P, double* G, int mode) -> int {
     cudaEvent_t a, b;
@@ -358,7 +397,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     cudaEventRecord(a, s);
     int rc2;
     if (o->df) {
-      rc2 = df_jk_device(e, C.p, nocc, mode, J.p, K.p, s);
+      rc2 = df_jk_device(e, Cuse, nocc, mode, J.p, K.p, s);
       if (mode == 1) ++mixed_builds;
       if (!rc2) {
         g.copy(J.p, G, nn);
@@ -406,6 +445,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
       g.copy(F.p, Finc.p, nn);
     } else {
       int rc2 = JK_OK;
+      if (mixed && switched) align();
       if (!switched) {
         rc2 = jk(nullptr, t2.p, 1);
       } else if (mixed && (!have_delta || since_refresh >= refresh_every)) {
