@@ -126,11 +126,12 @@ typedef struct jk_scf_options {
   int nocc;
   int df;                  /* 0 = integral-direct J/K, 1 = density-fitted */
   int prec_mode;           /* DF only: 0 = FP64; 1 = split-BF16 tensor-core builds while
-                              ||D - D_old||_F >= mixed_switch, then mixed builds plus an
-                              FP64 correction G64 - Gmixed taken at the switch density,
-                              and the energy from a final FP64 build */
+                              ||D - D_old||_F >= mixed_switch and still falling, FP64
+                              builds to convergence after that */
   double mixed_switch;     /* default 1e-3; the switch also happens when ||dD|| stalls */
-  int mixed_refresh;       /* iterations between FP64 refreshes of the correction, default 4 */
+  int mixed_refresh;       /* 0 (default): FP64 builds after the switch.  k > 0: mixed builds
+                              plus the correction G64 - Gmixed refreshed every k iterations,
+                              energy from a final FP64 build */
   int eig_mode;            /* 0 = cuSOLVER syevd every iteration; 1 = Jacobi (syevj) on the
                               Fock matrix in the previous eigenvectors after the first */
   int maxiter;             /* molecular2 default 40 */

@@ -278,14 +278,16 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   int builds = 0, mixed_builds = 0, corrected_builds = 0;
   // Mixed precision (DF only): split-BF16 builds until ||dD|| < mixed_switch
   // or the density change stalls (no halving over three iterations: the floor
-  // set by the mixed builds' own error).  From then on one FP64 build and one
-  // mixed build at the same density give the correction Delta = G64 - Gmixed,
-  // refreshed every mixed_refresh iterations, and the other iterations use
-  // Gmixed(D) + Delta, whose error scales with |D - D_refresh| instead of |D|.
-  // The reported energy comes from a final FP64 build at the converged density.
+  // set by the mixed builds' own error), FP64 builds after that.  With
+  // mixed_refresh > 0 the later iterations instead use Gmixed(D) + Delta, where
+  // Delta = G64 - Gmixed is taken from one FP64 and one mixed build at the same
+  // density every mixed_refresh iterations, and the reported energy comes from a
+  // final FP64 build at the converged density.
   const bool mixed = o->df && o->prec_mode == 1;
   const double mixed_switch = o->mixed_switch > 0.0 ? o->mixed_switch : 1e-3;
-  const int refresh_every = o->mixed_refresh > 0 ? o->mixed_refresh : 4;
+  const int refresh_every = o->mixed_refresh > 0 ? o->mixed_refresh : 0;
+  const bool corrected = mixed && refresh_every > 0;
+  int fp64_after_switch = 0;
   bool switched = !mixed, have_delta = false;
   int since_refresh = 0, refreshes = 0;
   double dd_hist[3] = {1e300, 1e300, 1e300};
@@ -445,10 +447,10 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
       g.copy(F.p, Finc.p, nn);
     } else {
       int rc2 = JK_OK;
-      if (mixed && switched) align();
+      if (corrected && switched) align();
       if (!switched) {
         rc2 = jk(nullptr, t2.p, 1);
-      } else if (mixed && (!have_delta || since_refresh >= refresh_every)) {
+      } else if (corrected && (!have_delta || since_refresh >= refresh_every)) {
         if ((rc2 = jk(nullptr, Delta.p, 1))) return rc2;
         if ((rc2 = jk(nullptr, t2.p, 0))) return rc2;
         g.scal(-1.0, Delta.p, nn);
@@ -456,13 +458,14 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
         have_delta = true;
         since_refresh = 0;
         ++refreshes;
-      } else if (mixed) {
+      } else if (corrected) {
         if ((rc2 = jk(nullptr, t2.p, 1))) return rc2;
         g.axpy(1.0, Delta.p, t2.p, nn);
         ++corrected_builds;
         ++since_refresh;
       } else {
         rc2 = jk(nullptr, t2.p, 0);
+        if (mixed) ++fp64_after_switch;
       }
       if (rc2) return rc2;
       g.copy(H.p, F.p, nn);
@@ -539,18 +542,20 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     delta = std::fabs(energy - last_energy);
     if (it > 2) average(weights);
     transform(F.p);
-    // a mixed run only converges once its builds carry the FP64 correction
-    converged = dd < o->densconverge && delta < o->enconverge && (!mixed || (have_delta && refreshes >= 2));
+    // a mixed run converges only on FP64 (or FP64-corrected) builds
+    const bool precise = !mixed || (corrected ? (have_delta && refreshes >= 2) : fp64_after_switch >= 2);
+    converged = dd < o->densconverge && delta < o->enconverge && precise;
     ++it;
   }
   if (mixed) {
     int rc2 = df_mixed_error(e);
     if (rc2) return cleanup(), rc2;
-    // energy of the converged density with an FP64 Fock build
-    if ((rc2 = jk(nullptr, t2.p, 0))) return cleanup(), rc2;
-    g.copy(H.p, F.p, nn);
-    g.axpy(1.0, t2.p, F.p, nn);
-    calc_e();
+    if (corrected) {  // energy of the converged density with an FP64 Fock build
+      if ((rc2 = jk(nullptr, t2.p, 0))) return cleanup(), rc2;
+      g.copy(H.p, F.p, nn);
+      g.axpy(1.0, t2.p, F.p, nn);
+      calc_e();
+    }
   }
   if (!diagonalise()) return cleanup(), set_error(e, JK_ERR_CUDA, "syevd(F)");
   st = cudaStreamSynchronize(s);

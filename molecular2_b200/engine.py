@@ -203,7 +203,7 @@ class IntegralEngine:
 
     def scf_rhf(self, nocc, enuc, df=False, prec_mode=0, maxiter=40, maxdiis=8, diis=True, precision=1e-12,
                 enconverge=1e-7, densconverge=1e-4, guess_fock=None, want=False, mixed_switch=1e-3, eig_mode=0,
-                mixed_refresh=4):
+                mixed_refresh=0):
         """SCF::rhf on the device; returns (SCFResult, extras dict)."""
         n = self.n
         o = SCFOptions()

@@ -51,9 +51,9 @@ def test_mixed_scf_energy_within_1e6():
     mol = geometry.water_cluster(4, 6.0, seed=5)
     obs, aux = BasisSet(mol, "cc-pvdz"), BasisSet(mol, "vdz-jkfit")
     eng = _engine(obs, aux)
-    r64, _ = eng.scf_rhf(mol.nocc, mol.enuc(), df=True, densconverge=1e-7, enconverge=1e-9, maxiter=60)
+    r64, _ = eng.scf_rhf(mol.nocc, mol.enuc(), df=True, densconverge=1e-7, enconverge=1e-9, maxiter=80)
     rmx, _ = eng.scf_rhf(mol.nocc, mol.enuc(), df=True, prec_mode=1, densconverge=1e-7, enconverge=1e-9,
-                         maxiter=60)
+                         maxiter=80)
     print(f"SCF FP64 {r64.energy:.10f} ({r64.iterations} it), mixed {rmx.energy:.10f} "
           f"({rmx.iterations} it, {rmx.mixed_builds} mixed builds)")
     assert r64.converged and rmx.converged
