@@ -82,6 +82,23 @@ int jk_direct(jk_engine* e, const double* D, double precision, double multiplier
 int jk_direct_device(jk_engine* e, const double* dD, double precision, double multiplier, double* dJ,
                      double* dK, void* stream);
 
+/* Integral-direct J and K exactly as jk_direct_device, for callers that must
+ * not allocate device memory while building a Fock matrix: for example a
+ * service that reserves all device memory for a caching allocator at start-up
+ * and may not take more, or code running next to latency-sensitive streams,
+ * where cudaMalloc/cudaFree (which can synchronise the whole device) would
+ * stall them.  This call allocates nothing: its scratch is one fixed array in
+ * device memory that every GPU loading this library keeps until the process
+ * exits, which limits the basis to at most 512 Cartesian functions and 256
+ * shells (larger bases return JK_ERR_ARG; use jk_direct_device).  The engine
+ * itself is still created by jk_create, which does allocate.  The first call on
+ * a device looks up the array's device address, so make one call before any
+ * stream capture.  All calls share the array: calls whose GPU work overlaps
+ * (other streams, other engines on the same device) race and give wrong
+ * results; serialise them.  No counterpart in molecular2. */
+int jk_direct_noalloc(jk_engine* e, const double* dD, double precision, double multiplier, double* dJ,
+                      double* dK, void* stream);
+
 /* Number of shell quartets the last direct build evaluated. */
 long long jk_last_quartets(const jk_engine* e);
 

@@ -19,6 +19,7 @@
 // D is transformed to Cartesian functions first and J, K back afterwards.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -206,11 +207,105 @@ int direct_jk_device(jk_engine* e, const double* dD, double precision, double mu
   return check_cuda(e, cudaGetLastError(), "jk_direct launch");
 }
 
+// ---------------------------------------------------------------- no-allocation variant
+// Scratch of jk_direct_noalloc: one fixed array in device global memory.  Every
+// GPU that loads this library holds it (6.8 MB) until the process exits, and
+// every call on a device shares it.  Layout (in doubles): Cartesian D, J, K
+// (NOALLOC_MAX_CART^2 each), the shell-block norms (NOALLOC_MAX_SHELLS^2), then
+// Dmax and the quartet counter.
+constexpr int NOALLOC_MAX_CART = 512;
+constexpr int NOALLOC_MAX_SHELLS = 256;
+constexpr size_t NOALLOC_CC = (size_t)NOALLOC_MAX_CART * NOALLOC_MAX_CART;
+constexpr size_t NOALLOC_SS = (size_t)NOALLOC_MAX_SHELLS * NOALLOC_MAX_SHELLS;
+constexpr size_t NOALLOC_DOUBLES = 3 * NOALLOC_CC + NOALLOC_SS + 2;
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
+
+// Device address of the scratch array on `device`, looked up once per device
+// with that device current (the host-side symbol is not a device address).
+static cudaError_t noalloc_scratch(int device, double** out) {
+  static std::mutex mu;
+  static std::vector<double*> addr;
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)addr.size() <= device) addr.resize(device + 1, nullptr);
+  if (!addr[device]) {
+    int prev = -1;
+    cudaError_t st = cudaGetDevice(&prev);
+    if (st == cudaSuccess && prev != device) st = cudaSetDevice(device);
+    double* p = nullptr;
+    if (st == cudaSuccess) st = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+    if (prev >= 0 && prev != device) cudaSetDevice(prev);
+    if (st != cudaSuccess) return st;
+    addr[device] = p;
+  }
+  *out = addr[device];
+  return cudaSuccess;
+}
+
+int direct_jk_noalloc(jk_engine* e, const double* dD, double precision, double mult, double* dJ, double* dK,
+                      cudaStream_t s) {
+  const int nc = e->obs.n_cart, ns = e->obs.nshell;
+  if (nc > NOALLOC_MAX_CART || ns > NOALLOC_MAX_SHELLS)
+    return set_error(e, JK_ERR_ARG,
+                     "jk_direct_noalloc: basis too large for the fixed scratch (" + std::to_string(nc) +
+                         " Cartesian functions, max " + std::to_string(NOALLOC_MAX_CART) + "; " + std::to_string(ns) +
+                         " shells, max " + std::to_string(NOALLOC_MAX_SHELLS) + "); use jk_direct_device");
+  double* base = nullptr;
+  cudaError_t st = noalloc_scratch(e->device, &base);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_direct_noalloc: cudaGetSymbolAddress");
+  double* Dc = base;
+  double* Jc = base + NOALLOC_CC;
+  double* Kc = base + 2 * NOALLOC_CC;
+  double* Dn = base + 3 * NOALLOC_CC;
+  double* Dmax = Dn + NOALLOC_SS;
+  unsigned long long* counter = reinterpret_cast<unsigned long long*>(Dmax + 1);
+  // the array keeps the previous call's contents: clear the accumulators
+  launch_shell_norms(e, dD, Dn, Dmax, s);  // zeroes Dmax itself
+  launch_final_to_cart(e, dD, Dc, s);
+  cudaMemsetAsync(Jc, 0, sizeof(double) * nc * nc, s);
+  cudaMemsetAsync(Kc, 0, sizeof(double) * nc * nc, s);
+  cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+  JKParams P{};
+  P.pp = prim_view(e);
+  P.sh = shell_view(e);
+  P.Dnorm = Dn;
+  P.nshell = ns;
+  P.Dmax = Dmax;
+  P.Dc = Dc;
+  P.nc = nc;
+  P.Jc = Jc;
+  P.Kc = Kc;
+  P.precision = precision;
+  P.boys = e->boys.p;
+  P.counter = counter;
+  P.kchunk = 512;
+  for (int A = 0; A < NPAIRCLASS; ++A)
+    for (int B = 0; B <= A; ++B) {
+      const PairClassDev& bra = e->pcls[A];
+      const PairClassDev& ket = e->pcls[B];
+      if (bra.npair == 0 || ket.npair == 0) continue;
+      P.bra = view(bra);
+      P.ket = view(ket);
+      P.same_class = (A == B);
+      launch_jk(A, B, P, bra.npair, ket.npair, s);
+    }
+  launch_cart_to_final_sym(e, Jc, 0.25 * mult, dJ, s);
+  launch_cart_to_final_sym(e, Kc, 0.125 * mult, dK, s);
+  return check_cuda(e, cudaGetLastError(), "jk_direct_noalloc launch");
+}
+
 }  // namespace m2
 
 using namespace m2;
 
 extern "C" {
+
+int jk_direct_noalloc(jk_engine* e, const double* dD, double precision, double multiplier, double* dJ, double* dK,
+                      void* stream) {
+  if (!e || !dD || !dJ || !dK) return JK_ERR_ARG;
+  if (!(precision >= 0.0)) return set_error(e, JK_ERR_ARG, "jk_direct_noalloc: precision must be >= 0");
+  cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+  return direct_jk_noalloc(e, dD, precision, multiplier, dJ, dK, s);
+}
 
 int jk_direct_device(jk_engine* e, const double* dD, double precision, double multiplier, double* dJ, double* dK,
                      void* stream) {

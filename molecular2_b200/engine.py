@@ -36,6 +36,7 @@ SIGNATURES = {
     "jk_schwarz": (_I, [_P, _P]),
     "jk_direct": (_I, [_P, _P, _D, _D, _P, _P]),
     "jk_direct_device": (_I, [_P, _P, _D, _D, _P, _P, _P]),
+    "jk_direct_noalloc": (_I, [_P, _P, _D, _D, _P, _P, _P]),
     "jk_last_quartets": (ctypes.c_longlong, [_P]),
     "jk_eri3": (_I, [_P, _P]),
     "jk_eri2": (_I, [_P, _P]),
