@@ -179,6 +179,15 @@ typedef struct jk_scf_result {
 
 int jk_scf_rhf(jk_engine* e, const jk_scf_options* opt, jk_scf_result* res);
 
+/* RHF nuclear gradient dE/dx (natom x 3, atom-major) for the full density D
+ * and the energy-weighted density W = Cocc diag(eps_occ) Cocc^T (host, n x n):
+ * Fock::compute_forces (src/rhfgrad.cpp:15-89) = (T' + V') . D - 2 S' . W
+ * + 1/4 G'(D) . D + nuclear repulsion, with G' = compute_2body_fock_deriv<1>
+ * (src/rhfgrad.cpp:419-598) screened at `precision` over the overlap-screened
+ * shell-pair list.  The two-electron part alone is also written to grad2e
+ * when it is not NULL.  Needs jk_basis.atom. */
+int jk_grad_rhf(jk_engine* e, const double* D, const double* W, double precision, double* grad, double* grad2e);
+
 #ifdef __cplusplus
 }
 #endif

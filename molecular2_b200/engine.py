@@ -45,6 +45,7 @@ SIGNATURES = {
     "jk_df_device": (_I, [_P, _P, _I, _I, _P, _P, _P]),
     "jk_one_body": (_I, [_P, _P, _P, _P]),
     "jk_scf_rhf": (_I, [_P, _P, _P]),
+    "jk_grad_rhf": (_I, [_P, _P, _P, _D, _P, _P]),
     "jk_set_profiling": (_I, [_P, _I]),
     "jk_stage_ms": (_I, [_P, _P, _I, ctypes.POINTER(_I)]),
 }
@@ -184,6 +185,17 @@ class IntegralEngine:
     def jk_df_device(self, dC, nocc, dJ, dK, prec_mode=0, stream=None):
         self._check(self.lib.jk_df_device(self.h, ctypes.c_void_p(dC), nocc, prec_mode, ctypes.c_void_p(dJ),
                                           ctypes.c_void_p(dK), ctypes.c_void_p(stream) if stream else None))
+
+    # -- gradient --------------------------------------------------------------
+    def compute_forces(self, D, W, precision=1e-12):
+        """Fock::compute_forces: (gradient natom x 3, two-electron part natom x 3)."""
+        na = self.obs.mol.natom
+        D = np.asfortranarray(D, dtype=np.float64)
+        W = np.asfortranarray(W, dtype=np.float64)
+        g = np.zeros(3 * na)
+        g2 = np.zeros(3 * na)
+        self._check(self.lib.jk_grad_rhf(self.h, _p(D), _p(W), precision, _p(g), _p(g2)))
+        return g.reshape(na, 3), g2.reshape(na, 3)
 
     def set_profiling(self, on=True):
         self._check(self.lib.jk_set_profiling(self.h, 1 if on else 0))
