@@ -130,6 +130,17 @@ int jk_df_device(jk_engine* e, const double* dCocc, int nocc, int prec_mode, dou
 int jk_set_profiling(jk_engine* e, int on);
 int jk_stage_ms(jk_engine* e, float* ms, int nmax, int* nwritten);
 
+/* Two-electron Fock contribution of a density D given in a second basis dbs
+ * (n_d x n_d, column-major; shell-diagonal blocks only when shelldiag != 0):
+ *   G(1,2) = sum_{3,4 in dbs} 2 D(3,4) (12|34) - D(3,4) (13|24),  n x n over obs,
+ * screened at `precision`.  Replaces Fock::compute_2body_fock_general
+ * (src/fockbuild.cpp:477-583) as used by the SOAD guess
+ * (Fock::compute_soad_guess, src/fock.cpp:174-225, with dbs = STO-3G and D the
+ * spherically averaged atomic occupations times 0.5).  Needs no engine: it
+ * builds a temporary one on `device` for the union of both bases. */
+int jk_fock_general(const jk_basis* obs, const jk_basis* dbs, const double* D, int shelldiag, double precision,
+                    int device, double* G);
+
 /* Overlap, kinetic and nuclear-attraction matrices (point charges of
  * jk_create): IntegralEngine::compute_1body_ints (src/integrals.cpp:394-449). */
 int jk_one_body(jk_engine* e, double* S, double* T, double* V);

@@ -285,6 +285,9 @@ int one_body_device(jk_engine* e, double* S, double* T, double* V, cudaStream_t 
   cudaError_t st = Z.upload(e->Z, s);
   if (st == cudaSuccess) st = C.upload(e->atom_xyz, s);
   if (st != cudaSuccess) return check_cuda(e, st, "one_body upload");
+  // shell pairs whose primitive products all vanish are not in the pair
+  // lists; their blocks are zero, not whatever the buffers held before
+  for (double* M : {S, T, V}) cudaMemsetAsync(M, 0, sizeof(double) * (size_t)n * n, s);
   for (int pc = 0; pc < NPAIRCLASS; ++pc) {
     if (!e->pcls[pc].npair) continue;
     OneBodyParams P{};

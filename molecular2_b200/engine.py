@@ -46,6 +46,7 @@ SIGNATURES = {
     "jk_one_body": (_I, [_P, _P, _P, _P]),
     "jk_scf_rhf": (_I, [_P, _P, _P]),
     "jk_grad_rhf": (_I, [_P, _P, _P, _D, _P, _P]),
+    "jk_fock_general": (_I, [_P, _P, _P, _I, _D, _I, _P]),
     "jk_set_profiling": (_I, [_P, _I]),
     "jk_stage_ms": (_I, [_P, _P, _I, ctypes.POINTER(_I)]),
 }
@@ -93,6 +94,21 @@ def _p(a):
 
 def _bp(basis):
     return ctypes.cast(ctypes.pointer(basis.struct()), ctypes.c_void_p)
+
+
+def fock_general(obs: BasisSet, dbs: BasisSet, D, shelldiag=True, precision=1e-12, device=0):
+    """Fock::compute_2body_fock_general (src/fockbuild.cpp:477-583): G over obs
+    from the density D given in basis dbs."""
+    lib = load_library()
+    n = obs.nbf
+    D = np.asfortranarray(D, dtype=np.float64)
+    if D.shape != (dbs.nbf, dbs.nbf):
+        raise ValueError("D must be dbs.nbf x dbs.nbf")
+    G = np.zeros((n, n), order="F")
+    rc = lib.jk_fock_general(_bp(obs), _bp(dbs), _p(D), 1 if shelldiag else 0, precision, device, _p(G))
+    if rc:
+        raise JKError(rc, "jk_fock_general failed")
+    return G
 
 
 class IntegralEngine:
@@ -214,11 +230,27 @@ class IntegralEngine:
         self._check(self.lib.jk_one_body(self.h, _p(S), _p(T), _p(V)))
         return S, T, V
 
+    def soad_fock(self, precision=1e-12):
+        """Fock::compute_soad_guess (src/fock.cpp:174-225): H + G[D_SOAD], with
+        D_SOAD the STO-3G atomic occupations of the molecule."""
+        from .basis import sto3g_density
+        mol = self.obs.mol
+        _, T, V = self.one_body()
+        G = fock_general(self.obs, BasisSet(mol, "sto-3g", spherical=False), sto3g_density(mol),
+                         shelldiag=True, precision=precision)
+        return T + V + G
+
     def scf_rhf(self, nocc, enuc, df=False, prec_mode=0, maxiter=40, maxdiis=8, diis=True, precision=1e-12,
                 enconverge=1e-7, densconverge=1e-4, guess_fock=None, want=False, mixed_switch=1e-3, eig_mode=0,
-                mixed_refresh=0):
-        """SCF::rhf on the device; returns (SCFResult, extras dict)."""
+                mixed_refresh=0, guess="core"):
+        """SCF::rhf on the device; returns (SCFResult, extras dict).  guess is
+        "core" (core Hamiltonian) or "soad" (SOAD Fock, the reference default);
+        an explicit guess_fock overrides it."""
         n = self.n
+        if guess_fock is None and guess == "soad":
+            guess_fock = self.soad_fock(precision)
+        elif guess not in ("core", "soad"):
+            raise ValueError("guess must be 'core' or 'soad'")
         o = SCFOptions()
         o.nocc, o.df, o.prec_mode, o.maxiter, o.maxdiis, o.diis = nocc, int(df), prec_mode, maxiter, maxdiis, int(diis)
         o.mixed_switch, o.eig_mode, o.mixed_refresh = mixed_switch, eig_mode, mixed_refresh

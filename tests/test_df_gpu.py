@@ -67,3 +67,21 @@ def test_one_body(spherical):
     Sr, Tr, Vr = oracle.one_body(b)
     for X, Xr in ((S, Sr), (T, Tr), (V, Vr)):
         assert np.max(np.abs(X - Xr)) < 1e-11
+
+
+def test_one_body_on_reused_memory():
+    """One-body matrices are complete on device memory that held other data:
+    shell pairs with no significant primitive product are written as zeros."""
+    import torch
+    from molecular2_b200.engine import IntegralEngine
+    junk = torch.full((1 << 27,), float("nan"), dtype=torch.float64, device="cuda")
+    del junk
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    mol = geometry.water_cluster(8, 7.0, seed=8)
+    b = BasisSet(mol, "cc-pvdz")
+    S, T, V = IntegralEngine(b).one_body()
+    So, To, Vo = oracle.one_body(b)
+    assert np.max(np.abs(S - So)) < 1e-12
+    assert np.max(np.abs(T - To)) < 1e-11
+    assert np.max(np.abs(V - Vo)) < 1e-10

@@ -71,3 +71,24 @@ def test_gradient_central_differences():
             Es.append(r2.energy)
         fd = (Es[0] - Es[1]) / (2 * h)
         assert abs(fd - g[a, x]) < 1e-6, (a, x, fd, g[a, x])
+
+
+def test_autograd_shim():
+    """torch.autograd.Function over jk_scf_rhf / jk_grad_rhf: backward equals
+    compute_forces at the converged SCF and central differences of forward."""
+    import torch
+    from molecular2_b200.autograd import rhf_energy
+    mol = geometry.water_cluster(2, 5.0, seed=3)
+    x = torch.tensor(mol.xyz, dtype=torch.float64, requires_grad=True)
+    E = rhf_energy(x, mol.symbols, "cc-pvdz")
+    E.backward()
+    g = x.grad.numpy()
+    assert np.max(np.abs(g.sum(axis=0))) < 1e-9
+    h = 1e-4
+    for a, c in [(2, 0), (3, 1)]:
+        Es = []
+        for sgn in (1, -1):
+            xd = x.detach().clone()
+            xd[a, c] += sgn * h
+            Es.append(float(rhf_energy(xd, mol.symbols, "cc-pvdz")))
+        assert abs((Es[0] - Es[1]) / (2 * h) - g[a, c]) < 1e-6
