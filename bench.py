@@ -9,7 +9,10 @@ converged occupied orbitals; `value` is builds/s with everything resident in
 HBM, `e2e` the same through the host-pointer C entry point (C uploaded, J and
 K downloaded every step).  The whole RHF SCF is timed once per precision
 mode and reported under "scf" (mixed = split-BF16 tensor-core builds, then
-FP64 builds to convergence), with |dE| between the two.
+FP64 builds to convergence), with |dE| between the two.  Two more
+workloads are timed once and reported beside the line: the FP64 analytic
+gradient of (H2O)8/cc-pVDZ ("gradient") and one FP64 integral-direct J/K
+build of C20H42/6-311G** ("direct_jk"); --no-extras skips them.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision mixed|fp64] [--profile]
@@ -39,11 +42,26 @@ UNIT = "builds/s"
 SEED = 16
 
 
+_WORKLOAD = None
+
+
 def workload():
-    from molecular2_b200 import geometry
-    from molecular2_b200.basis import BasisSet
-    mol = geometry.water16(SEED)
-    return mol, BasisSet(mol, "cc-pvdz"), BasisSet(mol, "vdz-jkfit")
+    global _WORKLOAD
+    if _WORKLOAD is None:
+        from molecular2_b200 import geometry
+        from molecular2_b200.basis import BasisSet
+        mol = geometry.water16(SEED)
+        _WORKLOAD = (mol, BasisSet(mol, "cc-pvdz"), BasisSet(mol, "vdz-jkfit"))
+    return _WORKLOAD
+
+
+def traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu capture (None if absent)."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    k = json.load(open(p)).get("kernels", {}).get(kernel)
+    return k["dram_bytes_read"] + k["dram_bytes_write"] if k else None
 
 
 def config(mol, obs, aux, prec):
@@ -66,41 +84,58 @@ def peaks():
 # ---------------------------------------------------------------- CPU leg
 def cpu_sample(nthreads, target_s=12.0):
     """Time the naive per-iteration loops of compute_2body_fock_df on a
-    contiguous block of fitting functions; returns (builds/s, sample text)."""
+    contiguous block of fitting functions, doubling the block until one run
+    takes target_s / 3 (the whole sample stays within about target_s);
+    returns (builds/s extrapolated to all fitting functions, sample text, s)."""
     import oracle
     mol, obs, aux = workload()
     n, naux, nocc = obs.nbf, aux.nbf, mol.nocc
     rng = np.random.default_rng(0)
     npair = n * (n + 1) // 2
     C = np.asfortranarray(rng.normal(size=(n, nocc)))
+    Bfull = None
 
     def run(nk):
-        B = np.asfortranarray(rng.normal(size=(npair, nk)))
+        B = np.asfortranarray(Bfull[:, :nk])
         t = time.perf_counter()
         oracle.df_jk(B, C, (0, nk), nthreads=nthreads)
         return time.perf_counter() - t
 
-    t1, t2 = run(4), run(8)
-    per_k = max((t2 - t1) / 4.0, 1e-6)
-    nk = int(max(4, min(naux, target_s / per_k)))
-    t = run(nk)
-    builds_per_s = 1.0 / (t * naux / nk)
+    nk, prev, total = 2, None, 0.0
+    Bfull = np.asfortranarray(rng.normal(size=(npair, 2)))
+    while True:
+        if Bfull.shape[1] < nk:
+            Bfull = np.asfortranarray(rng.normal(size=(npair, nk)))
+        t = run(nk)
+        total += t
+        if t >= target_s / 3 or nk >= naux:
+            break
+        prev = (nk, t)
+        nk = min(naux, 2 * nk)
+    if prev is not None and t > prev[1]:
+        per_k = (t - prev[1]) / (nk - prev[0])          # slope, per fitting function
+        t_full = max(t + per_k * (naux - nk), t)
+    else:
+        t_full = t * naux / nk
     sample = (f"naive X/K/gamma/J loops of compute_2body_fock_df over {nk} of {naux} fitting functions "
-              f"(synthetic B values), {nthreads} thread(s), {t:.1f} s, extrapolated x{naux / nk:.1f}")
-    return builds_per_s, sample, t
+              f"(synthetic B values), {nthreads} thread(s), last run {t:.2f} s of {total:.1f} s sampled, "
+              f"extrapolated linearly to {naux}")
+    return 1.0 / t_full, sample, total
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     nthreads = os.cpu_count() or 1
+    # each step a bounded sample, sized so that warm-up + steps take about 2-3 minutes
+    per_step = min(3.0, max(0.3, 150.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
-        cpu_sample(nthreads, target_s=1.0)
+        cpu_sample(nthreads, target_s=per_step)
     vals = []
     t0 = time.perf_counter()
     sample = ""
     for _ in range(args.steps):
-        v, sample, _ = cpu_sample(nthreads, target_s=3.0)
+        v, sample, _ = cpu_sample(nthreads, target_s=per_step)
         vals.append(v)
     wall = time.perf_counter() - t0
     v = statistics.median(vals)
@@ -202,9 +237,80 @@ def roofline_mixed(n, naux, nocc, stages):
         ach = byts / stages[dom] / 1e6 if stages else None
         rl = {"kernel": names[dom], "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
               "frac": ach / hbm if ach else None, "algorithmic_bytes_per_launch": byts}
-    rl.update({"traffic": None, "peak_source": src, "stages": per,
+    kern = "k_gemm2" if dom == 1 else ("k_gemm1" if dom == 0 else "k_J_mixed")
+    rl.update({"traffic": traffic(kern), "traffic_source": "profiles/ncu_traffic.json (ncu dram bytes per launch)",
+               "peak_source": src, "stages": per,
                "stage_ms": {names[i]: round(float(stages[i]), 5) for i in range(len(stages))}})
     return rl
+
+
+# ---------------------------------------------------------------- other workloads
+def measure_gradient(local):
+    """RHF analytic gradient of (H2O)8/cc-pVDZ (n=192), FP64, after a direct
+    SCF from the SOAD guess: Fock::compute_forces (src/rhfgrad.cpp:15-89)."""
+    from molecular2_b200 import geometry
+    from molecular2_b200.basis import BasisSet
+    from molecular2_b200.engine import IntegralEngine
+    mol = geometry.water8()
+    eng = IntegralEngine(BasisSet(mol, "cc-pvdz"), device=local)
+    t = time.perf_counter()
+    r, ex = eng.scf_rhf(mol.nocc, mol.enuc(), guess="soad", want=True, densconverge=1e-8, enconverge=1e-10,
+                        maxiter=60)
+    scf_s = time.perf_counter() - t
+    C = ex["C"][:, :mol.nocc]
+    W = C @ np.diag(ex["eps"][:mol.nocc]) @ C.T
+    eng.compute_forces(ex["D"], W)
+    ts = []
+    for _ in range(3):
+        t = time.perf_counter()
+        g, _ = eng.compute_forces(ex["D"], W)
+        ts.append(time.perf_counter() - t)
+    eng.close()
+    return {"workload": f"(H2O)8 RHF/cc-pVDZ analytic nuclear gradient, FP64 direct (n=192, {mol.natom} atoms), "
+                        "seed 8, SOAD guess",
+            "scf_s": scf_s, "scf_iterations": r.iterations, "energy": r.energy,
+            "gradient_ms": 1e3 * statistics.median(ts), "timing": "host wall clock around jk_grad_rhf",
+            "max_abs_sum_g": float(np.abs(g.sum(axis=0)).max())}
+
+
+def measure_direct(local):
+    """One FP64 integral-direct J/K build of C20H42/6-311G** (n=612) for the
+    SOAD-guess density: Fock::formJKdirect (src/fockbuild.cpp:64-164)."""
+    import scipy.linalg as sl
+    import torch
+    from molecular2_b200 import geometry
+    from molecular2_b200.basis import BasisSet
+    from molecular2_b200.engine import IntegralEngine
+    mol = geometry.c20h42()
+    b = BasisSet(mol, "6-311g**")
+    eng = IntegralEngine(b, device=local)
+    S, _, _ = eng.one_body()
+    _, C = sl.eigh(eng.soad_fock(), S)
+    D = 2.0 * C[:, :mol.nocc] @ C[:, :mol.nocc].T
+    n = b.nbf
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        dD = torch.from_numpy(np.ascontiguousarray(D)).cuda()
+        dJ = torch.empty_like(dD)
+        dK = torch.empty_like(dD)
+    torch.cuda.synchronize()
+    build = lambda: eng.jk_direct_device(dD.data_ptr(), dJ.data_ptr(), dK.data_ptr(), 1e-12,
+                                         stream=stream.cuda_stream)
+    build()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nb = 3
+    ev0.record(stream)
+    for _ in range(nb):
+        build()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / nb
+    q = eng.last_quartets()
+    eng.close()
+    return {"workload": f"C20H42 RHF/6-311G** FP64 integral-direct J/K build (n={n}), seed 20, SOAD-guess density, "
+                        "Schwarz x density screen 1e-12",
+            "ms_per_build": ms, "quartets": q, "quartets_per_s": q / (ms * 1e-3)}
 
 
 # ---------------------------------------------------------------- GPU leg
@@ -225,7 +331,10 @@ def run_ours(args, rank, world, local):
         rng = np.random.default_rng(0)
         C, _ = np.linalg.qr(rng.normal(size=(n, nocc)))
     else:
-        # SCF in both modes (not part of the timed builds); the FP64 orbitals feed the builds
+        # SCF in both modes (not part of the timed builds); the FP64 orbitals feed the builds.
+        # One short untimed SCF first, so neither timed run pays the library's first-call setup.
+        eng.scf_rhf(nocc, mol.enuc(), df=True, maxiter=2)
+        eng.scf_rhf(nocc, mol.enuc(), df=True, prec_mode=1, maxiter=2)
         t = time.perf_counter()
         r64, ex = eng.scf_rhf(nocc, mol.enuc(), df=True, densconverge=1e-6, enconverge=1e-8, want=True)
         s64 = time.perf_counter() - t
@@ -325,6 +434,11 @@ def run_ours(args, rank, world, local):
     e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * nocc * 8,
            "d2h_bytes_per_step": 2 * n * n * 8, "timing": "host wall clock around synchronous calls"}
 
+    other = {}
+    if rank == 0 and not args.no_extras:
+        other["gradient"] = measure_gradient(local)
+        other["direct_jk"] = measure_direct(local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sample, _ = cpu_sample(1)
@@ -338,7 +452,7 @@ def run_ours(args, rank, world, local):
                 "data": "synthetic (seeded geometry; basis data from molecular2's library)",
                 "config": config(mol, obs, aux, args.precision), "e2e": e2e, "roofline": roofline,
                 "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches * args.steps, "scf": scf,
-                "df_setup_s": setup_s}
+                "df_setup_s": setup_s, **other}
         print(json.dumps(line), flush=True)
     eng.close()
 
@@ -352,6 +466,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--profile", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the gradient and direct J/K measurements")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
