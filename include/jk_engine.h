@@ -199,6 +199,20 @@ int jk_scf_rhf(jk_engine* e, const jk_scf_options* opt, jk_scf_result* res);
  * when it is not NULL.  Needs jk_basis.atom. */
 int jk_grad_rhf(jk_engine* e, const double* D, const double* W, double precision, double* grad, double* grad2e);
 
+/* RHF nuclear gradient of the density-fitted energy (the energy whose Fock
+ * matrix jk_df / Fock::formJKdf builds, src/fockbuild.cpp:585-660) for the
+ * occupied orbitals Cocc (host, n x nocc column-major) with energies eps_occ:
+ * (T' + V') . D - 2 S' . W + nuclear repulsion as Fock::compute_forces
+ * (src/rhfgrad.cpp:15-89), with D = 2 Cocc Cocc^T and W = Cocc diag(eps_occ)
+ * Cocc^T, plus the derivative of the fitted two-electron energy,
+ *   sum (mn|P)^x [c_P D_mn - 2 (C d^P C^T)_mn] + sum (P|Q)^x [d^P . d^Q - c_P c_Q / 2],
+ * c = V^-1 (P|mn) D_mn, d^P_ij = V^-1 (Q|ij).  The two-electron part alone
+ * goes to grad2e when it is not NULL.  Runs jk_df_setup first if needed; needs
+ * jk_basis.atom on both bases.  molecular2 has no DF gradient (its
+ * compute_forces differentiates the 4-index energy); this is the gradient
+ * the DF SCF energy needs. */
+int jk_grad_df(jk_engine* e, const double* Cocc, int nocc, const double* eps_occ, double* grad, double* grad2e);
+
 #ifdef __cplusplus
 }
 #endif

@@ -53,10 +53,35 @@ static void launch_grad2e(int A, int B, const Grad2eParams& P, int nbra, int nke
     launch_grad2e_bra_dd(B, P, grid, s);
 }
 
-// dD, dW final-basis n x n on the device; g2e/g1e (3*natom) device
-// accumulators, zeroed here.  Synchronises the stream before returning.
-int grad_rhf_device(jk_engine* e, const double* dD, const double* dW, double precision, double* g2e, double* g1e,
+void launch_scale_K(int n, const double* K, const double* p, const double* alpha, double* K2a, double* K2b,
                     cudaStream_t s) {
+  k_scale_K<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, K, p, alpha, K2a, K2b);
+}
+
+// dE_nuc/dx, natom x 3 (src/rhfgrad.cpp:59-86)
+void nuclear_repulsion_grad(const jk_engine* e, std::vector<double>& gn) {
+  const int na = e->natom;
+  gn.assign(3 * (size_t)na, 0.0);
+  for (int a1 = 1; a1 < na; ++a1)
+    for (int a2 = 0; a2 < a1; ++a2) {
+      double r[3], r2 = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        r[k] = e->atom_xyz[3 * a1 + k] - e->atom_xyz[3 * a2 + k];
+        r2 += r[k] * r[k];
+      }
+      const double f = e->Z[a1] * e->Z[a2] / (r2 * std::sqrt(r2));
+      for (int k = 0; k < 3; ++k) {
+        gn[3 * a1 + k] -= r[k] * f;
+        gn[3 * a2 + k] += r[k] * f;
+      }
+    }
+}
+
+// dD, dW final-basis n x n on the device; g2e/g1e (3*natom) device
+// accumulators, zeroed here (g2e only when with_2e).  Synchronises the stream
+// before returning.
+int grad_rhf_device(jk_engine* e, const double* dD, const double* dW, double precision, double* g2e, double* g1e,
+                    cudaStream_t s, bool with_2e) {
   const int n = e->obs.n_final, nc = e->obs.n_cart, ns = e->obs.nshell, na = e->natom;
   for (int k = 0; k < ns; ++k)
     if (e->obs.atom[k] < 0 || e->obs.atom[k] >= na)
@@ -90,7 +115,7 @@ int grad_rhf_device(jk_engine* e, const double* dD, const double* dW, double pre
   launch_shell_norms(e, dD, Dn.p, Dmax.p, s);
   launch_final_to_cart(e, dD, Dc.p, s);
   launch_final_to_cart(e, dW, Wc.p, s);
-  cudaMemsetAsync(g2e, 0, sizeof(double) * 3 * na, s);
+  if (with_2e) cudaMemsetAsync(g2e, 0, sizeof(double) * 3 * na, s);
   cudaMemsetAsync(g1e, 0, sizeof(double) * 3 * na, s);
   Grad2eParams P{};
   P.pp = prim_view(e);
@@ -109,7 +134,7 @@ int grad_rhf_device(jk_engine* e, const double* dD, const double* dW, double pre
   P.boys = e->boys.p;
   P.grad = g2e;
   P.kchunk = 256;
-  for (int A = 0; A < NPAIRCLASS; ++A)
+  for (int A = 0; A < NPAIRCLASS && with_2e; ++A)
     for (int B = 0; B <= A; ++B) {
       if (!e->pcls[A].npair || !e->pcls[B].npair) continue;
       P.bra = view(e->pcls[A]);
@@ -162,27 +187,14 @@ extern "C" int jk_grad_rhf(jk_engine* e, const double* D, const double* W, doubl
   if (st == cudaSuccess) st = cudaMemcpyAsync(dD.p, D, sizeof(double) * n * n, cudaMemcpyHostToDevice, e->stream);
   if (st == cudaSuccess) st = cudaMemcpyAsync(dW.p, W, sizeof(double) * n * n, cudaMemcpyHostToDevice, e->stream);
   if (st != cudaSuccess) return check_cuda(e, st, "jk_grad_rhf upload");
-  int rc = grad_rhf_device(e, dD.p, dW.p, precision, g2.p, g1.p, e->stream);
+  int rc = grad_rhf_device(e, dD.p, dW.p, precision, g2.p, g1.p, e->stream, true);
   if (rc) return rc;
   std::vector<double> h2(3 * na), h1(3 * na);
   st = cudaMemcpy(h2.data(), g2.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost);
   if (st == cudaSuccess) st = cudaMemcpy(h1.data(), g1.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost);
   if (st != cudaSuccess) return check_cuda(e, st, "jk_grad_rhf download");
-  // nuclear repulsion (src/rhfgrad.cpp:59-86)
-  std::vector<double> gn(3 * na, 0.0);
-  for (int a1 = 1; a1 < na; ++a1)
-    for (int a2 = 0; a2 < a1; ++a2) {
-      double r[3], r2 = 0.0;
-      for (int k = 0; k < 3; ++k) {
-        r[k] = e->atom_xyz[3 * a1 + k] - e->atom_xyz[3 * a2 + k];
-        r2 += r[k] * r[k];
-      }
-      const double f = e->Z[a1] * e->Z[a2] / (r2 * std::sqrt(r2));
-      for (int k = 0; k < 3; ++k) {
-        gn[3 * a1 + k] -= r[k] * f;
-        gn[3 * a2 + k] += r[k] * f;
-      }
-    }
+  std::vector<double> gn;
+  nuclear_repulsion_grad(e, gn);
   for (int i = 0; i < 3 * na; ++i) grad[i] = h1[i] + h2[i] + gn[i];
   if (grad2e)
     for (int i = 0; i < 3 * na; ++i) grad2e[i] = h2[i];

@@ -47,6 +47,7 @@ SIGNATURES = {
     "jk_scf_rhf": (_I, [_P, _P, _P]),
     "jk_grad_rhf": (_I, [_P, _P, _P, _D, _P, _P]),
     "jk_fock_general": (_I, [_P, _P, _P, _I, _D, _I, _P]),
+    "jk_grad_df": (_I, [_P, _P, _I, _P, _P, _P]),
     "jk_set_profiling": (_I, [_P, _I]),
     "jk_stage_ms": (_I, [_P, _P, _I, ctypes.POINTER(_I)]),
 }
@@ -211,6 +212,20 @@ class IntegralEngine:
         g = np.zeros(3 * na)
         g2 = np.zeros(3 * na)
         self._check(self.lib.jk_grad_rhf(self.h, _p(D), _p(W), precision, _p(g), _p(g2)))
+        return g.reshape(na, 3), g2.reshape(na, 3)
+
+    def compute_forces_df(self, Cocc, eps_occ):
+        """Gradient of the density-fitted RHF energy for occupied orbitals
+        Cocc (n x nocc) and their energies: (gradient natom x 3, two-electron
+        part natom x 3)."""
+        na = self.obs.mol.natom
+        C = np.asfortranarray(Cocc, dtype=np.float64)
+        eps = np.ascontiguousarray(eps_occ, dtype=np.float64)
+        if eps.shape != (C.shape[1],):
+            raise ValueError("eps_occ must have one entry per occupied orbital")
+        g = np.zeros(3 * na)
+        g2 = np.zeros(3 * na)
+        self._check(self.lib.jk_grad_df(self.h, _p(C), C.shape[1], _p(eps), _p(g), _p(g2)))
         return g.reshape(na, 3), g2.reshape(na, 3)
 
     def set_profiling(self, on=True):
