@@ -117,6 +117,15 @@ int jk_eri2(jk_engine* e, double* V);
  * HBM.  Returns JK_ERR_NOT_PD when the metric is not positive definite. */
 int jk_df_setup(jk_engine* e);
 
+/* Keep only the fitted functions k0 <= K < k1 of B (call before jk_df_setup):
+ * jk_df then returns this slice's partial J and K, and the sum over slices
+ * that cover 0..naux is the full build (one all-reduce per build when ranks
+ * hold the slices).  Every slice still computes the full (P|mn) and the
+ * Cholesky factor once at set-up.  The DF SCF and jk_grad_df need the whole
+ * range (JK_ERR_STATE otherwise).  Replaces nothing in molecular2, whose DF
+ * build is serial (src/fockbuild.cpp:621-659). */
+int jk_df_set_range(jk_engine* e, int k0, int k1);
+
 /* Per-iteration part of compute_2body_fock_df (src/fockbuild.cpp:621-659):
  * J and K with respect to Cocc Cocc^T (the caller forms mult*(2J - K) as
  * Fock::formJKdf does at :173).  prec_mode 0 = FP64.  Host pointers. */

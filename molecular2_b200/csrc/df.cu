@@ -193,11 +193,13 @@ int df_setup(jk_engine* e) {
   cudaStream_t s = e->stream;
   const int n = e->obs.n_final, naux = e->aux.n_final;
   DFState& d = e->df;
+  const int k0 = d.k0, k1 = d.k1 < 0 ? naux : d.k1, nloc = k1 - k0;
+  if (k0 < 0 || k1 > naux || nloc <= 0) return set_error(e, JK_ERR_ARG, "DF range outside the fitting basis");
   DevBuf<double> T3, Linv;
   cudaError_t st = T3.alloc((size_t)n * naux * n);
   if (st == cudaSuccess) st = d.L.alloc((size_t)naux * naux);
   if (st == cudaSuccess) st = Linv.alloc((size_t)naux * naux);
-  if (st == cudaSuccess) st = d.B64.alloc((size_t)n * naux * n);
+  if (st == cudaSuccess) st = d.B64.alloc((size_t)n * nloc * n);
   if (st != cudaSuccess) return check_cuda(e, st, "df_setup allocation");
   if ((rc = compute_T3(e, T3.p, s))) return rc;
   if ((rc = compute_V(e, d.L.p, s))) return rc;
@@ -229,14 +231,14 @@ int df_setup(jk_engine* e) {
   if (cublasDtrsm(e->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, naux,
                   naux, &one, d.L.p, naux, Linv.p, naux) != CUBLAS_STATUS_SUCCESS)
     return set_error(e, JK_ERR_CUDA, "trsm for L^-1");
-  // B[x]^T (n x naux, ld n) = T[x]^T (n x naux) . Linv^T
-  if (cublasDgemmStridedBatched(e->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n, naux, naux, &one, T3.p, n,
-                                (long long)naux * n, Linv.p, naux, 0, &zero, d.B64.p, n, (long long)naux * n,
+  // B[x]^T (n x nloc, ld n) = T[x]^T (n x naux) . (rows k0..k1 of Linv)^T
+  if (cublasDgemmStridedBatched(e->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n, nloc, naux, &one, T3.p, n,
+                                (long long)naux * n, Linv.p + k0, naux, 0, &zero, d.B64.p, n, (long long)nloc * n,
                                 n) != CUBLAS_STATUS_SUCCESS)
     return set_error(e, JK_ERR_CUDA, "B = T L^-T gemm");
   st = cudaStreamSynchronize(s);
   if (st != cudaSuccess) return check_cuda(e, st, "df_setup");
-  d.naux = naux;
+  d.naux = nloc;
   d.ready = true;
   return JK_OK;
 }
@@ -356,6 +358,16 @@ int jk_eri2(jk_engine* e, double* V) {
 int jk_df_setup(jk_engine* e) {
   if (!e) return JK_ERR_ARG;
   return df_setup(e);
+}
+
+int jk_df_set_range(jk_engine* e, int k0, int k1) {
+  if (!e) return JK_ERR_ARG;
+  if (e->df.ready) return set_error(e, JK_ERR_STATE, "jk_df_set_range after jk_df_setup");
+  const int naux = e->has_aux ? e->aux.n_final : 0;
+  if (k0 < 0 || k1 <= k0 || k1 > naux) return set_error(e, JK_ERR_ARG, "jk_df_set_range: need 0 <= k0 < k1 <= naux");
+  e->df.k0 = k0;
+  e->df.k1 = k1;
+  return JK_OK;
 }
 
 int jk_df_device(jk_engine* e, const double* dC, int nocc, int prec_mode, double* dJ, double* dK, void* stream) {

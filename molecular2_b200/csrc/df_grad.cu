@@ -194,6 +194,8 @@ extern "C" int jk_grad_df(jk_engine* e, const double* Cocc, int nocc, const doub
   if (!e || !Cocc || !eps_occ || !grad) return JK_ERR_ARG;
   const int n = e->obs.n_final, na = e->natom;
   if (nocc <= 0 || nocc > n) return set_error(e, JK_ERR_ARG, "jk_grad_df: nocc out of range");
+  if (e->df.k0 != 0 || (e->df.k1 >= 0 && e->df.k1 != e->aux.n_final))
+    return set_error(e, JK_ERR_STATE, "jk_grad_df needs the whole fitting range (jk_df_set_range)");
   if (!e->df.ready) {
     int rc = df_setup(e);
     if (rc) return rc;

@@ -80,7 +80,8 @@ struct PairClassDev {
 
 struct DFState {
   bool ready = false;
-  int naux = 0;
+  int naux = 0;             // fitted functions held here (k1 - k0)
+  int k0 = 0, k1 = -1;      // fitted-index range kept in HBM (k1 < 0: all)
   DevBuf<double> B64;      // [x][K][y] unpacked, FP64
   DevBuf<double> L;        // Cholesky factor of the metric (naux x naux, col-major)
   DevBuf<double> X64;      // [x][K][i]

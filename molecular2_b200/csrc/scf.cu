@@ -208,6 +208,8 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   const int n = e->obs.n_final, nocc = o->nocc;
   const size_t nn = (size_t)n * n;
   if (nocc <= 0 || nocc > n) return set_error(e, JK_ERR_ARG, "scf: nocc out of range");
+  if (o->df && (e->df.k0 != 0 || (e->df.k1 >= 0 && e->df.k1 != e->aux.n_final)))
+    return set_error(e, JK_ERR_STATE, "scf: the DF SCF needs the whole fitting range (jk_df_set_range)");
   if (o->df && !e->df.ready) {
     int rc = df_setup(e);
     if (rc) return rc;

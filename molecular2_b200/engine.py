@@ -41,6 +41,7 @@ SIGNATURES = {
     "jk_eri3": (_I, [_P, _P]),
     "jk_eri2": (_I, [_P, _P]),
     "jk_df_setup": (_I, [_P]),
+    "jk_df_set_range": (_I, [_P, _I, _I]),
     "jk_df": (_I, [_P, _P, _I, _I, _P, _P]),
     "jk_df_device": (_I, [_P, _P, _I, _I, _P, _P, _P]),
     "jk_one_body": (_I, [_P, _P, _P, _P]),
@@ -189,6 +190,19 @@ class IntegralEngine:
 
     def df_setup(self):
         self._check(self.lib.jk_df_setup(self.h))
+
+    @property
+    def df_range(self):
+        return getattr(self, "_df_range", (0, self.naux))
+
+    def set_df_range(self, k0, k1):
+        """Keep only fitted functions k0 <= K < k1 (before df_setup); jk_df then
+        gives this slice's partial J, K.  An empty range builds nothing."""
+        if k0 == k1:
+            self._df_range = (k0, k1)
+            return
+        self._check(self.lib.jk_df_set_range(self.h, k0, k1))
+        self._df_range = (k0, k1)
 
     def jk_df(self, Cocc, prec_mode=0):
         """J, K with respect to Cocc Cocc^T (compute_2body_fock_df)."""

@@ -85,3 +85,30 @@ def test_one_body_on_reused_memory():
     assert np.max(np.abs(S - So)) < 1e-12
     assert np.max(np.abs(T - To)) < 1e-11
     assert np.max(np.abs(V - Vo)) < 1e-10
+
+
+@pytest.mark.parametrize("prec_mode", [0, 1])
+def test_df_slices_sum_to_full_build(prec_mode):
+    """jk_df_set_range: the partial J, K of fitted-index slices covering the
+    fitting basis add up to the one-engine build (the aux-sharded build that
+    bench.py runs over ranks, here two slices on one GPU)."""
+    from molecular2_b200.engine import IntegralEngine
+    from molecular2_b200.sharding import aux_ranges
+    mol = geometry.water_cluster(2, 5.0, seed=3)
+    obs, aux = BasisSet(mol, "cc-pvdz"), BasisSet(mol, "vdz-jkfit")
+    rng = np.random.default_rng(2)
+    C = np.linalg.qr(rng.normal(size=(obs.nbf, mol.nocc)))[0]
+    full = IntegralEngine(obs, aux)
+    full.df_setup()
+    J1, K1 = full.jk_df(C, prec_mode)
+    J2, K2 = np.zeros_like(J1), np.zeros_like(K1)
+    for k0, k1 in aux_ranges(aux.nbf, 2):
+        e = IntegralEngine(obs, aux)
+        e.set_df_range(k0, k1)
+        e.df_setup()
+        J, K = e.jk_df(C, prec_mode)
+        J2 += J
+        K2 += K
+    tol = 1e-11 if prec_mode == 0 else 5e-5 * np.abs(K1).max()
+    assert np.max(np.abs(J2 - J1)) < tol
+    assert np.max(np.abs(K2 - K1)) < tol
