@@ -37,9 +37,10 @@ __device__ __forceinline__ void sph_index_adj(const double* in, double* out, int
 }
 
 // quartet_cart kept out of line for the derivative classes: inlined into
-// k_grad3, ptxas (CUDA 12.9, -O3) produced wrong (P|m n+-1) integrals for the
-// fitting classes d and f with p-p orbital pairs, while a host build of the
-// same source agrees with finite differences of the integrals.
+// k_grad3, the CUDA 12.9 build (with ptxas -O3 and with -O0 alike) gave wrong
+// contributions for the fitting classes d and f with p-p orbital pairs, while
+// a host build of the same source and this out-of-line form both agree with
+// finite differences of the integrals.
 template <int LA, int LB, int LC, int LD>
 __device__ __noinline__ void quartet_cart_ool(const PrimView& pp, int b0, int nb, double Ax, double Ay, double Az,
                                               double Bx, double By, double Bz, const PrimView& kp, int k0, int nk,
@@ -109,26 +110,26 @@ __global__ void __launch_bounds__(64) k_grad3(const Grad3Params P) {
   double gM[3] = {0, 0, 0}, gN[3] = {0, 0, 0};
   {
     double I[NP * ncart(LM + 1) * NN];
-    quartet_cart_ool<LP, 0, LM + 1, LN>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp2a, kp0, knp, Ax, Ay, Az, Bx, By, Bz,
-                                    P.boys, I);
+    quartet_cart_ool<LP, 0, LM + 1, LN>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp2a, kp0, knp, Ax, Ay, Az, Bx,
+                                        By, Bz, P.boys, I);
     contract_shift<LP, 0, LM, LN, 2, 1>(I, Wt, gM);
   }
   if constexpr (LM > 0) {
     double I[NP * ncart(LM - 1) * NN];
-    quartet_cart_ool<LP, 0, LM - 1, LN>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp, kp0, knp, Ax, Ay, Az, Bx, By, Bz,
-                                    P.boys, I);
+    quartet_cart_ool<LP, 0, LM - 1, LN>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp, kp0, knp, Ax, Ay, Az, Bx, By,
+                                        Bz, P.boys, I);
     contract_shift<LP, 0, LM, LN, 2, -1>(I, Wt, gM);
   }
   {
     double I[NP * NM * ncart(LN + 1)];
-    quartet_cart_ool<LP, 0, LM, LN + 1>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp2b, kp0, knp, Ax, Ay, Az, Bx, By, Bz,
-                                    P.boys, I);
+    quartet_cart_ool<LP, 0, LM, LN + 1>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp2b, kp0, knp, Ax, Ay, Az, Bx,
+                                        By, Bz, P.boys, I);
     contract_shift<LP, 0, LM, LN, 3, 1>(I, Wt, gN);
   }
   if constexpr (LN > 0) {
     double I[NP * NM * ncart(LN - 1)];
-    quartet_cart_ool<LP, 0, LM, LN - 1>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp, kp0, knp, Ax, Ay, Az, Bx, By, Bz,
-                                    P.boys, I);
+    quartet_cart_ool<LP, 0, LM, LN - 1>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp, kp0, knp, Ax, Ay, Az, Bx, By,
+                                        Bz, P.boys, I);
     contract_shift<LP, 0, LM, LN, 3, -1>(I, Wt, gN);
   }
   // the sum over ordered (m, n) counts an off-diagonal canonical pair twice
