@@ -61,8 +61,48 @@ struct G1Layout {
   static constexpr int TMEM_COLS = 2 * ACC_STRIDE;
 };
 
+// One epilogue warp's share of a GEMM1 tile: TMEM columns [16*C0, 16*C1) of
+// its 32 rows.  Releases the accumulator buffer as soon as the values are in
+// registers, then adds this share to gamma and writes X as BF16 hi/lo.
+template <int NP, int C0, int C1>
+__device__ __forceinline__ void g1_epilogue_part(uint32_t taddr, int m, const G1Params& P, uint64_t* tempty_b,
+                                                 int lane) {
+  constexpr int NV = (C1 - C0) * 16;
+  float v[NV > 0 ? NV : 1];
+#pragma unroll
+  for (int c = C0; c < C1; ++c) tmem_ld16(taddr + c * 16, v + (c - C0) * 16);
+  if constexpr (NV > 0) tmem_ld_wait();
+  tc_fence_before();
+  __syncwarp();
+  if (lane == 0) mbar_arrive(tempty_b);
+  if (NV == 0 || m >= P.M) return;
+  const int x = m / P.naux, K = m - x * P.naux;
+  const double* Cx = P.C + x;
+  double g4[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int i = 0; i < NV; ++i)
+    if (C0 * 16 + i < P.nocc) g4[i & 3] += (double)v[i] * __ldg(Cx + (size_t)(C0 * 16 + i) * P.n);
+  atomicAdd(P.gamma + K, (g4[0] + g4[1]) + (g4[2] + g4[3]));
+  uint4* oh = reinterpret_cast<uint4*>(P.Xhi + (size_t)m * NP + C0 * 16);
+  uint4* ol = reinterpret_cast<uint4*>(P.Xlo + (size_t)m * NP + C0 * 16);
+#pragma unroll
+  for (int c = 0; c < NV / 8; ++c) {
+    __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const float f = v[c * 8 + e];
+      h[e] = __float2bfloat16_rn(f);
+      l[e] = __float2bfloat16_rn(f - __bfloat162float(h[e]));
+    }
+    oh[c] = *reinterpret_cast<const uint4*>(h);
+    ol[c] = *reinterpret_cast<const uint4*>(l);
+  }
+}
+
+constexpr int G1_THREADS = 320;  // TMA warp, MMA warp, 8 epilogue warps (2 per TMEM lane quadrant)
+
 template <int NP>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(G1_THREADS, 1)
     k_gemm1(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
             const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl, const G1Params P) {
   using Lay = G1Layout<NP>;
@@ -84,7 +124,7 @@ __global__ void __launch_bounds__(192, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 4);
+      mbar_init(&tempty[b], 8);
     }
     mbar_init(drain, 1);
     fence_barrier_init();
@@ -165,8 +205,9 @@ __global__ void __launch_bounds__(192, 1)
       umma_commit(drain);  // every issued MMA has finished before TMEM is freed
       mbar_wait(drain, 0);
     }
-  } else {  // epilogue: warps 2..5 drain TMEM lanes 32*(warp%4) ..
-    const int q = warp & 3;
+  } else {  // epilogue: warps 2..9; warp w drains TMEM lanes 32*(w%4).. and half (w-2)/4 of the columns
+    const int q = warp & 3, half = (warp - 2) >> 2;
+    constexpr int NCH = NP / 16, CH0 = (NCH + 1) / 2;
     int lt = 0;
     for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++lt) {
       const int b = lt & 1;
@@ -176,35 +217,12 @@ __global__ void __launch_bounds__(192, 1)
         break;
       }
       tc_fence_after();
-      float v[NP];
       const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + b * Lay::ACC_STRIDE;
-#pragma unroll
-      for (int c = 0; c < NP / 16; ++c) tmem_ld16(taddr + c * 16, v + c * 16);
-      tmem_ld_wait();
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty[b]);
       const int m = t * BM + 32 * q + lane;
-      if (m < P.M) {
-        const int x = m / P.naux, K = m - x * P.naux;
-        double g = 0.0;
-        for (int i = 0; i < P.nocc; ++i) g += (double)v[i] * P.C[(size_t)i * P.n + x];
-        atomicAdd(P.gamma + K, g);
-        uint4* oh = reinterpret_cast<uint4*>(P.Xhi + (size_t)m * NP);
-        uint4* ol = reinterpret_cast<uint4*>(P.Xlo + (size_t)m * NP);
-#pragma unroll
-        for (int c = 0; c < NP / 8; ++c) {
-          __align__(16) __nv_bfloat16 h[8], l[8];
-#pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const float f = v[c * 8 + e];
-            h[e] = __float2bfloat16_rn(f);
-            l[e] = __float2bfloat16_rn(f - __bfloat162float(h[e]));
-          }
-          oh[c] = *reinterpret_cast<const uint4*>(h);
-          ol[c] = *reinterpret_cast<const uint4*>(l);
-        }
-      }
+      if (half == 0)
+        g1_epilogue_part<NP, 0, CH0>(taddr, m, P, &tempty[b], lane);
+      else
+        g1_epilogue_part<NP, CH0, NCH>(taddr, m, P, &tempty[b], lane);
     }
   }
   tc_fence_before();
@@ -454,7 +472,7 @@ static cudaError_t launch_g1(const CUtensorMap* m, const G1Params& P, int grid, 
   using Lay = G1Layout<NP>;
   cudaError_t st = cudaFuncSetAttribute(k_gemm1<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, Lay::SMEM);
   if (st != cudaSuccess) return st;
-  k_gemm1<NP><<<grid, 192, Lay::SMEM, s>>>(m[0], m[1], m[2], m[3], P);
+  k_gemm1<NP><<<grid, G1_THREADS, Lay::SMEM, s>>>(m[0], m[1], m[2], m[3], P);
   return cudaGetLastError();
 }
 
