@@ -99,7 +99,8 @@ __device__ __forceinline__ void g1_epilogue_part(uint32_t taddr, int m, const G1
   }
 }
 
-constexpr int G1_THREADS = 320;  // TMA warp, MMA warp, 8 epilogue warps (2 per TMEM lane quadrant)
+constexpr int G1_EPI = 3;                            // epilogue warps per TMEM lane quadrant
+constexpr int G1_THREADS = 64 + 4 * 32 * G1_EPI;     // TMA warp, MMA warp, epilogue warps
 
 template <int NP>
 __global__ void __launch_bounds__(G1_THREADS, 1)
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&tfull[b], 1);
-      mbar_init(&tempty[b], 8);
+      mbar_init(&tempty[b], 4 * G1_EPI);
     }
     mbar_init(drain, 1);
     fence_barrier_init();
@@ -205,9 +206,10 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
       umma_commit(drain);  // every issued MMA has finished before TMEM is freed
       mbar_wait(drain, 0);
     }
-  } else {  // epilogue: warps 2..9; warp w drains TMEM lanes 32*(w%4).. and half (w-2)/4 of the columns
-    const int q = warp & 3, half = (warp - 2) >> 2;
-    constexpr int NCH = NP / 16, CH0 = (NCH + 1) / 2;
+  } else {  // epilogue: warp w drains TMEM lanes 32*(w%4).. and part (w-2)/4 of the 16-column chunks
+    const int q = warp & 3, part = (warp - 2) >> 2;
+    constexpr int NCH = NP / 16;
+    constexpr int CH1 = (NCH + G1_EPI - 1) / G1_EPI, CH2 = (2 * NCH + G1_EPI - 1) / G1_EPI;
     int lt = 0;
     for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++lt) {
       const int b = lt & 1;
@@ -219,10 +221,13 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
       tc_fence_after();
       const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + b * Lay::ACC_STRIDE;
       const int m = t * BM + 32 * q + lane;
-      if (half == 0)
-        g1_epilogue_part<NP, 0, CH0>(taddr, m, P, &tempty[b], lane);
+      static_assert(G1_EPI == 3, "chunk split below is written for three parts");
+      if (part == 0)
+        g1_epilogue_part<NP, 0, CH1>(taddr, m, P, &tempty[b], lane);
+      else if (part == 1)
+        g1_epilogue_part<NP, CH1, CH2>(taddr, m, P, &tempty[b], lane);
       else
-        g1_epilogue_part<NP, CH0, NCH>(taddr, m, P, &tempty[b], lane);
+        g1_epilogue_part<NP, CH2, NCH>(taddr, m, P, &tempty[b], lane);
     }
   }
   tc_fence_before();
