@@ -405,29 +405,53 @@ __global__ void k_split_C(int n, int nocc, int NP, int ldb, const double* __rest
   Cl[(size_t)i * ldb + y] = __float2bfloat16_rn((float)(dv - (double)__bfloat162float(h)));
 }
 
-// J[x][y] += sum_{K in chunk} gamma_K (Bhi + Blo)[x][K][y] for y <= x (8 y per thread)
-__global__ void k_J_mixed(int n, int naux, int ldb, int kchunk, const __nv_bfloat16* __restrict__ Bh,
-                          const __nv_bfloat16* __restrict__ Bl, const double* __restrict__ gamma,
-                          double* __restrict__ J) {
+// J[x][y] += sum_{K in [K0, K1)} gamma_K (Bhi + Blo)[x][K][y] for y <= x.
+// One block per (x, K range): the ny = ceil((x+1)/8) threads of a K group
+// read 8 consecutive y each (16-byte loads of one row of B), and the block's
+// remaining threads form further K groups, so short rows (small x) still keep
+// the whole block busy.  Partial sums meet in shared memory; one atomic per
+// (x, y) per block.
+constexpr int JM_THREADS = 256;
+__global__ void __launch_bounds__(JM_THREADS) k_J_mixed(int n, int naux, int ldb, int kchunk,
+                                                        const __nv_bfloat16* __restrict__ Bh,
+                                                        const __nv_bfloat16* __restrict__ Bl,
+                                                        const double* __restrict__ gamma, double* __restrict__ J) {
+  __shared__ float part[JM_THREADS * 8];
   const int x = blockIdx.x;
-  const int y0 = threadIdx.x * 8;
-  if (y0 > x) return;
+  const int ny_all = (x + 8) / 8;                  // y groups of 8 covering 0..x
   const int K0 = blockIdx.y * kchunk, K1 = min(naux, K0 + kchunk);
-  float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  const size_t base = (size_t)x * naux * ldb + y0;
+  const int t = threadIdx.x;
+  for (int yb = 0; yb < ny_all; yb += JM_THREADS) {   // one pass unless x >= 8 * JM_THREADS
+    const int ny = min(ny_all - yb, JM_THREADS);
+    const int ngroups = JM_THREADS / ny;               // K groups
+    const int yi = t % ny, kg = t / ny;
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (kg < ngroups) {
+      const size_t base = (size_t)x * naux * ldb + (size_t)(yb + yi) * 8;
 #pragma unroll 4
-  for (int K = K0; K < K1; ++K) {
-    const float g = (float)__ldg(gamma + K);
-    const uint4 hv = __ldg(reinterpret_cast<const uint4*>(Bh + base + (size_t)K * ldb));
-    const uint4 lv = __ldg(reinterpret_cast<const uint4*>(Bl + base + (size_t)K * ldb));
-    const __nv_bfloat16* h = reinterpret_cast<const __nv_bfloat16*>(&hv);
-    const __nv_bfloat16* l = reinterpret_cast<const __nv_bfloat16*>(&lv);
+      for (int K = K0 + kg; K < K1; K += ngroups) {
+        const float g = (float)__ldg(gamma + K);
+        const uint4 hv = __ldg(reinterpret_cast<const uint4*>(Bh + base + (size_t)K * ldb));
+        const uint4 lv = __ldg(reinterpret_cast<const uint4*>(Bl + base + (size_t)K * ldb));
+        const __nv_bfloat16* h = reinterpret_cast<const __nv_bfloat16*>(&hv);
+        const __nv_bfloat16* l = reinterpret_cast<const __nv_bfloat16*>(&lv);
 #pragma unroll
-    for (int e = 0; e < 8; ++e) acc[e] += g * (__bfloat162float(h[e]) + __bfloat162float(l[e]));
+        for (int e = 0; e < 8; ++e) acc[e] += g * (__bfloat162float(h[e]) + __bfloat162float(l[e]));
+      }
+    }
+    __syncthreads();  // the previous pass's readers are done with part[]
+#pragma unroll
+    for (int e = 0; e < 8; ++e) part[t * 8 + e] = acc[e];
+    __syncthreads();
+    // the first ny*8 threads each sum the K groups of one y = 8 (yb + yy) + e
+    for (int idx = t; idx < ny * 8; idx += JM_THREADS) {
+      const int yy = idx / 8, e = idx % 8, y = (yb + yy) * 8 + e;
+      if (y > x || y >= n) continue;
+      float sum = 0.0f;
+      for (int k = 0; k < ngroups; ++k) sum += part[(k * ny + yy) * 8 + e];
+      atomicAdd(J + (size_t)y * n + x, (double)sum);
+    }
   }
-#pragma unroll
-  for (int e = 0; e < 8; ++e)
-    if (y0 + e <= x && y0 + e < n) atomicAdd(J + (size_t)(y0 + e) * n + x, (double)acc[e]);
 }
 
 // J: mirror the lower triangle; K: assemble from the lower-triangle tiles of Kt
@@ -579,9 +603,9 @@ int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double
   st = cudaGetLastError();
   if (st != cudaSuccess) return check_cuda(e, st, "gemm2 launch");
   stage_mark(e, 2, s);
-  const int kchunk = 64;
-  k_J_mixed<<<dim3(n, (naux + kchunk - 1) / kchunk), (ldb + 7) / 8, 0, s>>>(n, naux, ldb, kchunk, m.Bh.p, m.Bl.p,
-                                                                            d.gamma.p, dJ);
+  const int kchunk = (naux + 7) / 8;   // 8 K ranges per row x
+  k_J_mixed<<<dim3(n, (naux + kchunk - 1) / kchunk), JM_THREADS, 0, s>>>(n, naux, ldb, kchunk, m.Bh.p, m.Bl.p,
+                                                                         d.gamma.p, dJ);
   stage_mark(e, 3, s);
   const size_t nn = (size_t)n * n;
   k_finalize_mixed<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(n, m.Kt.p, dJ, dK);
