@@ -603,7 +603,7 @@ int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double
   st = cudaGetLastError();
   if (st != cudaSuccess) return check_cuda(e, st, "gemm2 launch");
   stage_mark(e, 2, s);
-  const int kchunk = (naux + 7) / 8;   // 8 K ranges per row x
+  const int kchunk = (naux + 15) / 16;   // 16 K ranges per row x
   k_J_mixed<<<dim3(n, (naux + kchunk - 1) / kchunk), JM_THREADS, 0, s>>>(n, naux, ldb, kchunk, m.Bh.p, m.Bl.p,
                                                                          d.gamma.p, dJ);
   stage_mark(e, 3, s);
