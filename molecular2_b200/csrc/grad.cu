@@ -133,7 +133,7 @@ int grad_rhf_device(jk_engine* e, const double* dD, const double* dW, double pre
   P.precision = precision;
   P.boys = e->boys.p;
   P.grad = g2e;
-  P.kchunk = 256;
+  P.kchunk = 64;  // one ket per thread (64-thread blocks)
   for (int A = 0; A < NPAIRCLASS && with_2e; ++A)
     for (int B = 0; B <= A; ++B) {
       if (!e->pcls[A].npair || !e->pcls[B].npair) continue;

@@ -190,7 +190,7 @@ int direct_jk_device(jk_engine* e, const double* dD, double precision, double mu
   P.precision = precision;
   P.boys = e->boys.p;
   P.counter = counter;
-  P.kchunk = 512;
+  P.kchunk = 128;  // one ket per thread: small classes still spread over the SMs
   for (int A = 0; A < NPAIRCLASS; ++A)
     for (int B = 0; B <= A; ++B) {
       const PairClassDev& bra = e->pcls[A];
@@ -277,7 +277,7 @@ int direct_jk_noalloc(jk_engine* e, const double* dD, double precision, double m
   P.precision = precision;
   P.boys = e->boys.p;
   P.counter = counter;
-  P.kchunk = 512;
+  P.kchunk = 128;  // one ket per thread: small classes still spread over the SMs
   for (int A = 0; A < NPAIRCLASS; ++A)
     for (int B = 0; B <= A; ++B) {
       const PairClassDev& bra = e->pcls[A];
