@@ -41,7 +41,12 @@ __global__ void k_scale_K(int n, const double* __restrict__ K, const double* __r
   K2b[i] = 2.0 * (p[i] - alpha[i]) * K[i];
 }
 
-static void launch_grad2e(int A, int B, const Grad2eParams& P, int nbra, int nket, cudaStream_t s) {
+// kets per 64-thread block: one per thread, halved for classes with few bra
+// pairs so that their blocks still spread over the SMs
+static void launch_grad2e(int A, int B, const Grad2eParams& Pin, int nbra, int nket, cudaStream_t s) {
+  Grad2eParams P = Pin;
+  P.kchunk = 64;
+  if ((long long)nbra * ((nket + 63) / 64) < 4 * 148) P.kchunk = 32;
   dim3 grid(nbra, (nket + P.kchunk - 1) / P.kchunk);
   if (A <= 2)
     launch_grad2e_bra_s(A, B, P, grid, s);

@@ -147,7 +147,19 @@ int build_pairs(jk_engine* e) {
   return check_cuda(e, st, "schwarz matrix");
 }
 
-static void launch_jk(int A, int B, const JKParams& P, int nbra, int nket_max, cudaStream_t s) {
+// Kets per block: one per thread (128) when the class has enough (bra, chunk)
+// blocks to fill the GPU; classes with few bra pairs take smaller chunks so
+// their work still spreads over about 4 blocks per SM (idle threads of a
+// block only cost its residency).
+static int ket_chunk(int nbra, int nket_max) {
+  int k = 128;
+  while (k > 32 && (long long)nbra * ((nket_max + k - 1) / k) < 4 * 148) k /= 2;
+  return k;
+}
+
+static void launch_jk(int A, int B, const JKParams& Pin, int nbra, int nket_max, cudaStream_t s) {
+  JKParams P = Pin;
+  P.kchunk = ket_chunk(nbra, nket_max);
   dim3 grid(nbra, (nket_max + P.kchunk - 1) / P.kchunk);
   if (A <= 2)
     launch_jk_bra_s(A, B, P, grid, s);
