@@ -342,6 +342,27 @@ def measure_direct(local):
             "ms_per_build": ms, "quartets": q, "quartets_per_s": q / (ms * 1e-3)}
 
 
+def profile_direct(local):
+    """Two FP64 direct J/K builds of (H2O)8/cc-pVDZ at the density of one
+    diagonalisation of the SOAD Fock matrix (the ncu workload of the direct
+    classes)."""
+    import scipy.linalg as sl
+    from molecular2_b200 import geometry
+    from molecular2_b200.basis import BasisSet
+    from molecular2_b200.engine import IntegralEngine
+    mol = geometry.water8()
+    eng = IntegralEngine(BasisSet(mol, "cc-pvdz"), device=local)
+    S, _, _ = eng.one_body()
+    _, C = sl.eigh(eng.soad_fock(), S)
+    D = 2.0 * C[:, :mol.nocc] @ C[:, :mol.nocc].T
+    for _ in range(2):
+        t = time.perf_counter()
+        eng.jk_direct(D, 1e-12)
+        print(json.dumps({"profile_direct": True, "build_s": time.perf_counter() - t,
+                          "quartets": eng.last_quartets()}), flush=True)
+    eng.close()
+
+
 # ---------------------------------------------------------------- GPU leg
 def run_ours(args, rank, world, local):
     import torch
@@ -525,12 +546,17 @@ def main():
     ap.add_argument("--profile", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the gradient and direct J/K measurements")
+    ap.add_argument("--profile-direct", action="store_true",
+                    help="only two FP64 direct J/K builds of (H2O)8/cc-pVDZ at the SOAD-guess density (for ncu)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.profile_direct:
+        profile_direct(local)
         return
     if world > 1:
         import datetime
