@@ -193,9 +193,9 @@ class Clocks:
 
 
 def roofline_fp64(n, naux, nocc, stages):
-    names = ["X=B.C (cuBLAS DGEMM)", "K=X.X^T (cuBLAS DGEMM)", "gamma (k_gamma)", "J=B.gamma (k_df_J)"]
+    names = ["X=B.C (cuBLAS DGEMM)", "K=X.X^T (cuBLAS DGEMM)", "gamma (k_gamma)", "J=B.gamma (k_df_J_lower)"]
     hbm, bf16, src = peaks()
-    B_bytes = n * n * naux * 8
+    B_bytes = (n * (n + 1) // 2) * naux * 8   # k_df_J_lower reads the lower half of B
     own = 3
     ach = B_bytes / (stages[own] * 1e-3) / 1e9 if len(stages) > own else None
     return {"kernel": names[own], "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",

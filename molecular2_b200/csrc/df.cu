@@ -175,16 +175,63 @@ __global__ void k_gamma(int n, int naux, int o, const double* __restrict__ X, co
   }
 }
 
-// J[x][y] = sum_K gamma_K B[x][K][y]; one block per x, threads over y.
-__global__ void k_df_J(int n, int naux, const double* __restrict__ B, const double* __restrict__ g,
-                       double* __restrict__ J) {
+// J[x][y] += sum_{K in [K0, K1)} gamma_K B[x][K][y] for y <= x (FP64 B).
+// One block per (x, K range): ny = ceil((x+1)/2) threads of a K group read
+// two consecutive y each (16-byte loads of one row of B), the block's other
+// threads form further K groups, partial sums meet in shared memory and one
+// atomic per (x, y) and block goes to J.  Only the lower triangle of J is
+// written; k_mirror_lower fills the upper one.
+constexpr int DFJ_THREADS = 256;
+__global__ void __launch_bounds__(DFJ_THREADS) k_df_J_lower(int n, int naux, int kchunk,
+                                                            const double* __restrict__ B,
+                                                            const double* __restrict__ g, double* __restrict__ J) {
+  __shared__ double part[DFJ_THREADS * 2];
   const int x = blockIdx.x;
-  for (int y = threadIdx.x; y < n; y += blockDim.x) {
-    double acc = 0.0;
-    const double* b = B + (size_t)x * naux * n + y;
-    for (int K = 0; K < naux; ++K) acc += __ldg(g + K) * b[(size_t)K * n];
-    J[(size_t)y * n + x] = acc;
+  const int ny_all = (x + 2) / 2;
+  const int K0 = blockIdx.y * kchunk, K1 = min(naux, K0 + kchunk);
+  const int t = threadIdx.x;
+  for (int yb = 0; yb < ny_all; yb += DFJ_THREADS) {
+    const int ny = min(ny_all - yb, DFJ_THREADS);
+    const int ngroups = DFJ_THREADS / ny;
+    const int yi = t % ny, kg = t / ny;
+    const int y = (yb + yi) * 2;
+    double a0 = 0.0, a1 = 0.0;
+    if (kg < ngroups) {
+      const double* b = B + (size_t)x * naux * n + y;
+      const bool pair = (y + 1 < n) && ((n & 1) == 0);   // 16-byte aligned pair
+#pragma unroll 4
+      for (int K = K0 + kg; K < K1; K += ngroups) {
+        const double gk = __ldg(g + K);
+        if (pair) {
+          const double2 v = __ldg(reinterpret_cast<const double2*>(b + (size_t)K * n));
+          a0 += gk * v.x;
+          a1 += gk * v.y;
+        } else {
+          a0 += gk * __ldg(b + (size_t)K * n);
+          if (y + 1 < n) a1 += gk * __ldg(b + (size_t)K * n + 1);
+        }
+      }
+    }
+    __syncthreads();
+    part[t * 2] = a0;
+    part[t * 2 + 1] = a1;
+    __syncthreads();
+    for (int idx = t; idx < ny * 2; idx += DFJ_THREADS) {
+      const int yy = idx / 2, e = idx % 2, yo = (yb + yy) * 2 + e;
+      if (yo > x || yo >= n) continue;
+      double sum = 0.0;
+      for (int k = 0; k < ngroups; ++k) sum += part[(k * ny + yy) * 2 + e];
+      atomicAdd(J + (size_t)yo * n + x, sum);
+    }
   }
+}
+
+// upper triangle of a column-major symmetric matrix from its lower triangle
+__global__ void k_mirror_lower(int n, double* J) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)n * n) return;
+  const int i = (int)(idx % n), j = (int)(idx / n);
+  if (i < j) J[idx] = J[(size_t)i * n + j];
 }
 
 int df_setup(jk_engine* e) {
@@ -276,7 +323,11 @@ int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ,
   stage_mark(e, 2, s);
   k_gamma<<<naux, 256, 0, s>>>(n, naux, nocc, d.X64.p, dC, d.gamma.p);
   stage_mark(e, 3, s);
-  k_df_J<<<n, 128, 0, s>>>(n, naux, d.B64.p, d.gamma.p, dJ);
+  cudaMemsetAsync(dJ, 0, sizeof(double) * n * n, s);
+  const int kchunk = (naux + 15) / 16;   // 16 K ranges per row x
+  k_df_J_lower<<<dim3(n, (naux + kchunk - 1) / kchunk), DFJ_THREADS, 0, s>>>(n, naux, kchunk, d.B64.p, d.gamma.p,
+                                                                              dJ);
+  k_mirror_lower<<<(unsigned)(((size_t)n * n + 255) / 256), 256, 0, s>>>(n, dJ);
   stage_mark(e, 4, s);
   return check_cuda(e, cudaGetLastError(), "jk_df launch");
 }
