@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(64) k_grad2e(const Grad2eParams P) {
   const double Qab = P.bra.Q[bra];
   const double Dmax = *P.Dmax;
   if (!(Qab * Dmax > 0.0)) return;
-  int nket = q_prefix(P.ket.Q, P.ket.npair, P.precision / (Qab * Dmax));
+  int nket = window_up(q_prefix(P.ket.Q, P.ket.npair, P.precision / (Qab * Dmax)), P.ket.npair);
   if (P.same_class) nket = min(nket, bra + 1);
   const int start = blockIdx.y * P.kchunk;
   if (start >= nket) return;

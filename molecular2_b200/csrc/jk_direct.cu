@@ -123,6 +123,13 @@ int build_pairs(jk_engine* e) {
     std::vector<int> order(d.npair);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return c.Q[x] > c.Q[y]; });
+    // inside windows of PAIR_WINDOW, longest contractions first (warps of
+    // kets with similar primitive counts; kernels round Q prefixes to windows)
+    for (size_t w0 = 0; w0 < order.size(); w0 += PAIR_WINDOW) {
+      const size_t w1 = std::min(order.size(), w0 + (size_t)PAIR_WINDOW);
+      std::stable_sort(order.begin() + w0, order.begin() + w1,
+                       [&](int x, int y) { return c.nprim[x] > c.nprim[y]; });
+    }
     PairClassHost sorted;
     for (int o : order) {
       sorted.sa.push_back(c.sa[o]);

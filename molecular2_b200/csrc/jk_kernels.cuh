@@ -187,6 +187,18 @@ struct JKParams {
   int kchunk;
 };
 
+// Pairs of a class are sorted by Schwarz bound Q descending and then, inside
+// consecutive windows of PAIR_WINDOW pairs, by contraction length, so that
+// the 32 kets of a warp have similar primitive counts.  The Q prefix of a
+// threshold is therefore rounded up to a whole window; the per-ket screen
+// drops the extra kets.  Every Q of a window is >= every Q of the next one,
+// so a binary search lands inside the window holding the cut; window_up
+// returns the end of the window containing index k (k itself included).
+constexpr int PAIR_WINDOW = 256;
+__device__ __forceinline__ int window_up(int k, int n) {
+  return min(n, (k / PAIR_WINDOW + 1) * PAIR_WINDOW);
+}
+
 // number of kets in [0, n) whose Q >= thr (Q sorted descending)
 __device__ __forceinline__ int q_prefix(const double* Q, int n, double thr) {
   int lo = 0, hi = n;
@@ -213,7 +225,7 @@ __global__ void __launch_bounds__(128) k_jk_direct(const JKParams P) {
   const double Qab = P.bra.Q[bra];
   const double Dmax = *P.Dmax;
   if (!(Qab * Dmax > 0.0)) return;
-  int nket = q_prefix(P.ket.Q, P.ket.npair, P.precision / (Qab * Dmax));
+  int nket = window_up(q_prefix(P.ket.Q, P.ket.npair, P.precision / (Qab * Dmax)), P.ket.npair);
   if (P.same_class) nket = min(nket, bra + 1);
   const int start = blockIdx.y * P.kchunk;
   if (start >= nket) return;
