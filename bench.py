@@ -30,6 +30,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -431,8 +432,7 @@ def run_ours(args, rank, world, local):
         dist.barrier()
     clocks = None
     if rank == 0 and not args.profile:
-        outdir = os.path.join(ROOT, "gpurun_out") if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp"
-        clocks = Clocks(local, os.path.join(outdir, f"clocks_rank{rank}.csv"))
+        clocks = Clocks(local, os.path.join(args.clock_dir or tempfile.gettempdir(), f"clocks_rank{rank}.csv"))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
@@ -544,6 +544,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--profile", action="store_true")
+    ap.add_argument("--clock-dir", default=None, help="where the nvidia-smi clock samples go (default: a temp dir)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the gradient and direct J/K measurements")
     ap.add_argument("--profile-direct", action="store_true",

@@ -95,11 +95,14 @@ int jk_direct_device(jk_engine* e, const double* dD, double precision, double mu
  * a device looks up the array's device address, so make one call before any
  * stream capture.  All calls share the array: calls whose GPU work overlaps
  * (other streams, other engines on the same device) race and give wrong
- * results; serialise them.  No counterpart in molecular2. */
+ * results; serialise them.  Call it with the engine's device current
+ * (JK_ERR_ARG otherwise): the array's address differs per GPU.  No
+ * counterpart in molecular2. */
 int jk_direct_noalloc(jk_engine* e, const double* dD, double precision, double multiplier, double* dJ,
                       double* dK, void* stream);
 
-/* Number of shell quartets the last direct build evaluated. */
+/* Number of shell quartets the last direct build (jk_direct, jk_direct_device
+ * or jk_direct_noalloc) evaluated; -1 before the first build. */
 long long jk_last_quartets(const jk_engine* e);
 
 /* Three-index integrals (P|mn) in molecular2's packed layout: column-major
@@ -125,6 +128,19 @@ int jk_df_setup(jk_engine* e);
  * range (JK_ERR_STATE otherwise).  Replaces nothing in molecular2, whose DF
  * build is serial (src/fockbuild.cpp:621-659). */
 int jk_df_set_range(jk_engine* e, int k0, int k1);
+
+/* Layout of the fitted tensor, chosen before jk_df_setup (molecular2 keeps one
+ * packed FP64 (n(n+1)/2) x naux matrix, src/fockbuild.cpp:598-619, which
+ * stops fitting in device memory near n = 2600, naux = 9600):
+ *   1  unpacked FP64 B[x][K][y] plus its split-BF16 copy (small systems);
+ *   2  tiled: B_K kept on and below the diagonal of a 128 x 128 function
+ *      tiling, split BF16 only (half the bytes of the packed FP64 matrix);
+ *      the FP64 build (prec_mode 0) then recomputes the three-index
+ *      integrals per build instead of reading B;
+ *   0  automatic (default): tiled when the unpacked path would not fit.
+ * jk_df_storage reports the layout in use (0 before set-up). */
+int jk_df_set_storage(jk_engine* e, int mode);
+int jk_df_storage(const jk_engine* e);
 
 /* Per-iteration part of compute_2body_fock_df (src/fockbuild.cpp:621-659):
  * J and K with respect to Cocc Cocc^T (the caller forms mult*(2J - K) as

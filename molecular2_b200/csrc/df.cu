@@ -11,13 +11,16 @@
 //   K          = X X^T                        is one SYRK over the n x (naux*o) matrix X,
 //   gamma_K    = sum_{x,i} X[x][K][i] C[x][i] and
 //   J[x][y]    = sum_K gamma_K B[x][K][y]     stream X and B once each.
-// B = T L^-T with V = L L^T is formed once per geometry by a strided-batched
-// GEMM with L^-1 (the reference's O(n^2 naux^2) transform at :610-618).
+// B = T L^-T with V = L L^T is formed once per geometry by a batched GEMM
+// with L^-1 (the reference's O(n^2 naux^2) transform at :610-618); the
+// Cholesky factor, L^-1 and every GEMM are this library's own FP64 kernels
+// (dense.cu).
 #include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
 
+#include "dense.cuh"
 #include "df_kernels.cuh"
 #include "engine.h"
 
@@ -26,7 +29,7 @@ namespace m2 {
 PrimView prim_view(const jk_engine* e);
 ShellView shell_view(const jk_engine* e);
 
-static int prepare_aux(jk_engine* e) {
+int prepare_aux(jk_engine* e) {
   if (!e->has_aux) return set_error(e, JK_ERR_STATE, "no fitting basis was given to jk_create");
   if (e->ap_p.p) return JK_OK;
   const HostBasis& a = e->aux;
@@ -64,6 +67,34 @@ static PrimView aux_view(const jk_engine* e) {
   return PrimView{e->ap_p.p, e->ap_x.p, e->ap_y.p, e->ap_z.p, e->ap_K.p};
 }
 
+// Launch parameters of the three-index kernels for fitting shells of angular
+// momentum l and orbital pair class pc.
+Eri3Params eri3_params(const jk_engine* e, int l, int pc) {
+  Eri3Params P{};
+  P.ap = aux_view(e);
+  P.aux_shells = e->aux_by_l[l].p;
+  P.naux_shells = e->aux_by_l_count[l];
+  P.aux_prim_off = e->aux_prim_off.p;
+  P.aux_nprim = e->daux.nprim.p;
+  P.ax = e->daux.x.p;
+  P.ay = e->daux.y.p;
+  P.az = e->daux.z.p;
+  P.aux_foff = e->daux.final_off.p;
+  P.aux_pure = e->daux.pure.p;
+  P.pairs = view(e->pcls[pc]);
+  P.pp = prim_view(e);
+  P.ox = e->dobs.x.p;
+  P.oy = e->dobs.y.p;
+  P.oz = e->dobs.z.p;
+  P.obs_foff = e->dobs.final_off.p;
+  P.obs_pure = e->dobs.pure.p;
+  P.sph = e->dobs.sph.p;
+  P.boys = e->boys.p;
+  P.n = e->obs.n_final;
+  P.naux = e->aux.n_final;
+  return P;
+}
+
 // T3[x][P][y] = (P|xy), full n x naux x n.
 static int compute_T3(jk_engine* e, double* T3, cudaStream_t s) {
   const int n = e->obs.n_final, naux = e->aux.n_final;
@@ -72,28 +103,7 @@ static int compute_T3(jk_engine* e, double* T3, cudaStream_t s) {
     if (!e->aux_by_l_count[l]) continue;
     for (int pc = 0; pc < NPAIRCLASS; ++pc) {
       if (!e->pcls[pc].npair) continue;
-      Eri3Params P{};
-      P.ap = aux_view(e);
-      P.aux_shells = e->aux_by_l[l].p;
-      P.naux_shells = e->aux_by_l_count[l];
-      P.aux_prim_off = e->aux_prim_off.p;
-      P.aux_nprim = e->daux.nprim.p;
-      P.ax = e->daux.x.p;
-      P.ay = e->daux.y.p;
-      P.az = e->daux.z.p;
-      P.aux_foff = e->daux.final_off.p;
-      P.aux_pure = e->daux.pure.p;
-      P.pairs = view(e->pcls[pc]);
-      P.pp = prim_view(e);
-      P.ox = e->dobs.x.p;
-      P.oy = e->dobs.y.p;
-      P.oz = e->dobs.z.p;
-      P.obs_foff = e->dobs.final_off.p;
-      P.obs_pure = e->dobs.pure.p;
-      P.sph = e->dobs.sph.p;
-      P.boys = e->boys.p;
-      P.n = n;
-      P.naux = naux;
+      Eri3Params P = eri3_params(e, l, pc);
       P.T3 = T3;
       if (l == 0) launch_eri3_l0(pc, P, s);
       if (l == 1) launch_eri3_l1(pc, P, s);
@@ -104,7 +114,7 @@ static int compute_T3(jk_engine* e, double* T3, cudaStream_t s) {
   return check_cuda(e, cudaGetLastError(), "eri3 launch");
 }
 
-static int compute_V(jk_engine* e, double* V, cudaStream_t s) {
+int compute_V(jk_engine* e, double* V, cudaStream_t s) {
   const int naux = e->aux.n_final;
   for (int lp = 0; lp <= MAX_L_AUX; ++lp)
     for (int lq = 0; lq <= lp; ++lq) {
@@ -143,16 +153,6 @@ __global__ void k_pack_T3(int n, int naux, const double* __restrict__ T3, double
   while ((size_t)(x + 1) * (x + 2) / 2 <= xy) ++x;
   const int y = (int)(xy - (size_t)x * (x + 1) / 2);
   Tp[idx] = T3[((size_t)x * naux + P) * n + y];
-}
-
-__global__ void k_identity(int n, double* A) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < (size_t)n * n) A[i] = (i % (n + 1) == 0) ? 1.0 : 0.0;
-}
-
-__global__ void k_lower_only(int n, double* A) {  // zero the strict upper triangle (col-major)
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < (size_t)n * n && (int)(i % n) < (int)(i / n)) A[i] = 0.0;
 }
 
 // gamma_K = sum_{x,i} X[x][K][i] C[x][i]   (C column-major n x o)
@@ -234,9 +234,37 @@ __global__ void k_mirror_lower(int n, double* J) {
   if (i < j) J[idx] = J[(size_t)i * n + j];
 }
 
+// K (n x n, column-major) = X X^T for X given as n rows of length len
+// (row x at X + x*len): lower tiles split over the SMs, then mirrored.
+cudaError_t df_syrk_X(jk_engine* e, const double* X, int n, long long len, double* K, cudaStream_t s) {
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device);
+  const int tiles = ((n + 127) / 128) * ((n + 127) / 128 + 1) / 2;
+  const long long kt = (len + 15) / 16;
+  DGemm g;
+  g.M = n;
+  g.N = n;
+  g.K = (int)len;
+  g.A = X;
+  g.sam = len;
+  g.sak = 1;
+  g.B = X;
+  g.sbk = 1;
+  g.sbn = len;
+  g.C = K;
+  g.scm = 1;
+  g.scn = n;
+  g.c_lower = true;
+  g.ksplit = (int)std::max(1LL, std::min<long long>((2LL * nsm + tiles - 1) / tiles, kt / 8));
+  cudaError_t st = dgemm(g, s);
+  if (st == cudaSuccess) mirror_lower(K, n, s);
+  return st == cudaSuccess ? cudaGetLastError() : st;
+}
+
 int df_setup(jk_engine* e) {
   int rc = prepare_aux(e);
   if (rc) return rc;
+  if (df_use_tiled(e)) return df_tiled_setup(e);
   cudaStream_t s = e->stream;
   const int n = e->obs.n_final, naux = e->aux.n_final;
   DFState& d = e->df;
@@ -250,39 +278,45 @@ int df_setup(jk_engine* e) {
   if (st != cudaSuccess) return check_cuda(e, st, "df_setup allocation");
   if ((rc = compute_T3(e, T3.p, s))) return rc;
   if ((rc = compute_V(e, d.L.p, s))) return rc;
-  // V = L L^T (cuSOLVER potrf, lower)
-  int lwork = 0;
-  if (cusolverDnDpotrf_bufferSize(e->cusolver, CUBLAS_FILL_MODE_LOWER, naux, d.L.p, naux, &lwork) !=
-      CUSOLVER_STATUS_SUCCESS)
-    return set_error(e, JK_ERR_CUDA, "potrf buffer size");
+  // V = L L^T (own blocked Cholesky), then L^-1
   DevBuf<double> work;
   DevBuf<int> info;
-  st = work.alloc(lwork > 0 ? lwork : 1);
+  st = work.alloc((size_t)naux * naux);
   if (st == cudaSuccess) st = info.alloc(1);
-  if (st != cudaSuccess) return check_cuda(e, st, "potrf workspace");
-  if (cusolverDnDpotrf(e->cusolver, CUBLAS_FILL_MODE_LOWER, naux, d.L.p, naux, work.p, lwork, info.p) !=
-      CUSOLVER_STATUS_SUCCESS)
-    return set_error(e, JK_ERR_CUDA, "potrf");
+  if (st != cudaSuccess) return check_cuda(e, st, "Cholesky workspace");
+  if ((rc = cholesky(e, d.L.p, naux, work.p, info.p, s))) return rc;
   int hinfo = 0;
   st = cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (st == cudaSuccess) st = cudaStreamSynchronize(s);
-  if (st != cudaSuccess) return check_cuda(e, st, "potrf");
+  if (st != cudaSuccess) return check_cuda(e, st, "Cholesky");
   if (hinfo != 0)
     return set_error(e, JK_ERR_NOT_PD,
                      "fitting metric (P|Q) is not positive definite (leading minor " + std::to_string(hinfo) + ")");
-  const int nb = 256;
-  k_lower_only<<<(unsigned)(((size_t)naux * naux + nb - 1) / nb), nb, 0, s>>>(naux, d.L.p);
-  k_identity<<<(unsigned)(((size_t)naux * naux + nb - 1) / nb), nb, 0, s>>>(naux, Linv.p);
-  const double one = 1.0, zero = 0.0;
-  cublasSetStream(e->cublas, s);
-  if (cublasDtrsm(e->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, naux,
-                  naux, &one, d.L.p, naux, Linv.p, naux) != CUBLAS_STATUS_SUCCESS)
-    return set_error(e, JK_ERR_CUDA, "trsm for L^-1");
-  // B[x]^T (n x nloc, ld n) = T[x]^T (n x naux) . (rows k0..k1 of Linv)^T
-  if (cublasDgemmStridedBatched(e->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n, nloc, naux, &one, T3.p, n,
-                                (long long)naux * n, Linv.p + k0, naux, 0, &zero, d.B64.p, n, (long long)nloc * n,
-                                n) != CUBLAS_STATUS_SUCCESS)
-    return set_error(e, JK_ERR_CUDA, "B = T L^-T gemm");
+  if ((rc = tri_inverse(e, d.L.p, Linv.p, naux, work.p, s))) return rc;
+  // B[x] (nloc x n, y contiguous) = (rows k0..k1 of L^-1) . T[x]  for every x
+  DGemm g;
+  g.M = nloc;
+  g.N = n;
+  g.K = naux;
+  g.batch = n;
+  g.A = Linv.p + k0;
+  g.sam = 1;
+  g.sak = naux;
+  g.a_lower = (k0 == 0);
+  g.B = T3.p;
+  g.sbk = n;
+  g.sbn = 1;
+  g.bsb = (long long)naux * n;
+  g.C = d.B64.p;
+  g.scm = n;
+  g.scn = 1;
+  g.bsc = (long long)nloc * n;
+  st = dgemm(g, s);
+  if (st != cudaSuccess) return check_cuda(e, st, "B = L^-1 T");
+  st = d.Linv.alloc((size_t)naux * naux);
+  if (st == cudaSuccess)
+    st = cudaMemcpyAsync(d.Linv.p, Linv.p, sizeof(double) * naux * naux, cudaMemcpyDeviceToDevice, s);
+  if (st != cudaSuccess) return check_cuda(e, st, "keep L^-1");
   st = cudaStreamSynchronize(s);
   if (st != cudaSuccess) return check_cuda(e, st, "df_setup");
   d.naux = nloc;
@@ -300,6 +334,7 @@ void stage_mark(jk_engine* e, int k, cudaStream_t s) {
 
 int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ, double* dK, cudaStream_t s) {
   DFState& d = e->df;
+  if (e->tiled.ready) return df_tiled_device(e, dC, nocc, mode, dJ, dK, s);
   if (!d.ready) return set_error(e, JK_ERR_STATE, "jk_df before jk_df_setup");
   if (mode == 1) return df_mixed_device(e, dC, nocc, dJ, dK, s);
   if (mode != 0) return set_error(e, JK_ERR_ARG, "jk_df: unsupported precision mode");
@@ -307,19 +342,27 @@ int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ,
   cudaError_t st = d.X64.alloc((size_t)n * naux * nocc);
   if (st == cudaSuccess) st = d.gamma.alloc(naux);
   if (st != cudaSuccess) return check_cuda(e, st, "jk_df scratch");
-  const double one = 1.0, zero = 0.0;
-  cublasSetStream(e->cublas, s);
   stage_mark(e, 0, s);
-  // X (o x n*naux, col-major) = C^T . B   ->  X[x][K][i]
-  if (cublasDgemm(e->cublas, CUBLAS_OP_T, CUBLAS_OP_N, nocc, n * naux, n, &one, dC, n, d.B64.p, n, &zero, d.X64.p,
-                  nocc) != CUBLAS_STATUS_SUCCESS)
-    return set_error(e, JK_ERR_CUDA, "X = B C gemm");
+  // X[x][K][i] = sum_y B[x][K][y] C[y][i]: one GEMM over the n*naux rows (x, K)
+  DGemm gx;
+  gx.M = n * naux;
+  gx.N = nocc;
+  gx.K = n;
+  gx.A = d.B64.p;
+  gx.sam = n;
+  gx.sak = 1;
+  gx.B = dC;
+  gx.sbk = 1;
+  gx.sbn = n;
+  gx.C = d.X64.p;
+  gx.scm = nocc;
+  gx.scn = 1;
+  cudaError_t st2 = dgemm(gx, s);
+  if (st2 != cudaSuccess) return check_cuda(e, st2, "X = B C");
   stage_mark(e, 1, s);
-  // K = X^T X over the (naux*o) inner index (a full DGEMM: on this part
-  // cuBLAS DGEMM outruns DSYRK although it does twice the flops)
-  if (cublasDgemm(e->cublas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, naux * nocc, &one, d.X64.p, naux * nocc, d.X64.p,
-                  naux * nocc, &zero, dK, n) != CUBLAS_STATUS_SUCCESS)
-    return set_error(e, JK_ERR_CUDA, "K = X^T X gemm");
+  // K = X X^T over the (K, i) index: lower tiles, split over the SMs, mirrored
+  st2 = df_syrk_X(e, d.X64.p, n, (long long)naux * nocc, dK, s);
+  if (st2 != cudaSuccess) return check_cuda(e, st2, "K = X X^T");
   stage_mark(e, 2, s);
   k_gamma<<<naux, 256, 0, s>>>(n, naux, nocc, d.X64.p, dC, d.gamma.p);
   stage_mark(e, 3, s);

@@ -38,4 +38,15 @@ void launch_onebody(int pc, const OneBodyParams& P, cudaStream_t s) {
   if (pc == 5) k_onebody<2, 2><<<grid, 64, 0, s>>>(P);
 }
 
+
+void launch_eri3_tile_l0(int pc, const Eri3Params& P, const Eri3TileArgs& A, cudaStream_t s) {
+  dim3 grid((A.nlist + 63) / 64, P.naux_shells);
+  if (pc == 0) k_eri3_tile<0, 0, 0><<<grid, 64, 0, s>>>(P, A);
+  if (pc == 1) k_eri3_tile<0, 1, 0><<<grid, 64, 0, s>>>(P, A);
+  if (pc == 2) k_eri3_tile<0, 1, 1><<<grid, 64, 0, s>>>(P, A);
+  if (pc == 3) k_eri3_tile<0, 2, 0><<<grid, 64, 0, s>>>(P, A);
+  if (pc == 4) k_eri3_tile<0, 2, 1><<<grid, 64, 0, s>>>(P, A);
+  if (pc == 5) k_eri3_tile<0, 2, 2><<<grid, 64, 0, s>>>(P, A);
+}
+
 }  // namespace m2

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "df_grad_kernels.cuh"
+#include "dense.cuh"
 #include "engine.h"
 
 namespace m2 {
@@ -54,12 +55,20 @@ __global__ void k_scale_aux(int n, const double* __restrict__ K, const double* _
   if (i < n) K2[i] = 2.0 * p[i] * K[i];
 }
 
-static int cublas_fail(jk_engine* e, const char* what) { return set_error(e, JK_ERR_CUDA, what); }
+// Ce = C diag(eps), C column-major n x o
+__global__ void k_scale_cols(int n, int o, const double* __restrict__ C, const double* __restrict__ eps,
+                             double* __restrict__ Ce) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < (size_t)n * o) Ce[idx] = C[idx] * eps[idx / n];
+}
+
+int grad_df_2e_tiled(jk_engine* e, const double* dC, int nocc, const double* dD, double* g2e, cudaStream_t s);
 
 // dC: n x nocc column-major occupied orbitals; dD = 2 C C^T; g2e receives
 // the two-electron DF gradient (zeroed here).  Synchronises the stream.
 int grad_df_2e_device(jk_engine* e, const double* dC, int nocc, const double* dD, double* g2e, cudaStream_t s) {
   DFState& d = e->df;
+  if (e->tiled.ready) return grad_df_2e_tiled(e, dC, nocc, dD, g2e, s);
   const int n = e->obs.n_final, naux = d.naux, o = nocc, na = e->natom;
   const size_t nn = (size_t)n * n;
   for (int k = 0; k < e->aux.nshell; ++k)
@@ -75,36 +84,84 @@ int grad_df_2e_device(jk_engine* e, const double* dC, int nocc, const double* dD
   if (st == cudaSuccess) st = K2b.alloc(e->pp_p.n);
   if (st == cudaSuccess) st = ap2.alloc(e->ap_p.n);
   if (st != cudaSuccess) return check_cuda(e, st, "DF gradient allocation");
-  const double one = 1.0, zero = 0.0, mhalf = -0.5;
-  cublasSetStream(e->cublas, s);
-  cublasHandle_t h = e->cublas;
-  // X[x][K][i]: (o x n*naux) = C^T . B
-  if (cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, o, n * naux, n, &one, dC, n, d.B64.p, n, &zero, X.p, o) !=
-      CUBLAS_STATUS_SUCCESS)
-    return cublas_fail(e, "DF gradient: X = B C");
-  // bt[K] (o x o) = X_K (o x n, ld naux*o) . C (n x o)
-  if (cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, o, o, n, &one, X.p, naux * o, (long long)o, dC, n, 0,
-                                &zero, bt.p, o, (long long)o * o, naux) != CUBLAS_STATUS_SUCCESS)
-    return cublas_fail(e, "DF gradient: C^T X");
-  k_trace_bt<<<(naux + 127) / 128, 128, 0, s>>>(naux, o, bt.p, c.p);
-  // c = L^-T gt;  d = bt L^-1 (bt as o^2 x naux)
-  if (cublasDtrsv(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, naux, d.L.p, naux, c.p, 1) !=
-      CUBLAS_STATUS_SUCCESS)
-    return cublas_fail(e, "DF gradient: c = V^-1 gamma");
-  if (cublasDtrsm(h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, o * o, naux, &one,
-                  d.L.p, naux, bt.p, o * o) != CUBLAS_STATUS_SUCCESS)
-    return cublas_fail(e, "DF gradient: d = V^-1 b");
+  if (!d.Linv.p) return set_error(e, JK_ERR_STATE, "DF gradient: L^-1 missing (run jk_df_setup)");
+  DevBuf<double> dd, gt;
+  st = dd.alloc((size_t)o * o * naux);
+  if (st == cudaSuccess) st = gt.alloc(naux);
+  if (st != cudaSuccess) return check_cuda(e, st, "DF gradient allocation");
+  auto gemm = [&](const DGemm& g, const char* what) {
+    const cudaError_t r = dgemm(g, s);
+    return r == cudaSuccess ? JK_OK : check_cuda(e, r, what);
+  };
+  int rc;
+  // X[x][K][i] = sum_y B[x][K][y] C[y][i]
+  {
+    DGemm g;
+    g.M = n * naux; g.N = o; g.K = n;
+    g.A = d.B64.p; g.sam = n; g.sak = 1;
+    g.B = dC; g.sbk = 1; g.sbn = n;
+    g.C = X.p; g.scm = o; g.scn = 1;
+    if ((rc = gemm(g, "DF gradient: X = B C"))) return rc;
+  }
+  // bt[K](i, j) = sum_x X[x][K][i] C[x][j]   (o x o, column-major, per K)
+  {
+    DGemm g;
+    g.M = o; g.N = o; g.K = n; g.batch = naux;
+    g.A = X.p; g.sam = 1; g.sak = (long long)naux * o; g.bsa = o;
+    g.B = dC; g.sbk = 1; g.sbn = n;
+    g.C = bt.p; g.scm = 1; g.scn = o; g.bsc = (long long)o * o;
+    if ((rc = gemm(g, "DF gradient: C^T X"))) return rc;
+  }
+  k_trace_bt<<<(naux + 127) / 128, 128, 0, s>>>(naux, o, bt.p, gt.p);
+  // c = L^-T gamma
+  {
+    DGemm g;
+    g.M = naux; g.N = 1; g.K = naux;
+    g.A = d.Linv.p; g.sam = naux; g.sak = 1;
+    g.B = gt.p; g.sbk = 1; g.sbn = 0;
+    g.C = c.p; g.scm = 1; g.scn = 0;
+    if ((rc = gemm(g, "DF gradient: c = V^-1 gamma"))) return rc;
+  }
+  // d (o^2 x naux) = bt L^-1
+  {
+    DGemm g;
+    g.M = o * o; g.N = naux; g.K = naux;
+    g.A = bt.p; g.sam = 1; g.sak = (long long)o * o;
+    g.B = d.Linv.p; g.sbk = 1; g.sbn = naux; g.b_lower = true;
+    g.C = dd.p; g.scm = 1; g.scn = (long long)o * o;
+    if ((rc = gemm(g, "DF gradient: d = V^-1 b"))) return rc;
+  }
   // W2 = d^T d - 1/2 c c^T
-  if (cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, naux, naux, o * o, &one, bt.p, o * o, bt.p, o * o, &zero, W2.p,
-                  naux) != CUBLAS_STATUS_SUCCESS ||
-      cublasDger(h, naux, naux, &mhalf, c.p, 1, c.p, 1, W2.p, naux) != CUBLAS_STATUS_SUCCESS)
-    return cublas_fail(e, "DF gradient: W2");
+  {
+    DGemm g;
+    g.M = naux; g.N = naux; g.K = o * o;
+    g.A = dd.p; g.sam = (long long)o * o; g.sak = 1;
+    g.B = dd.p; g.sbk = 1; g.sbn = (long long)o * o;
+    g.C = W2.p; g.scm = 1; g.scn = naux;
+    if ((rc = gemm(g, "DF gradient: W2"))) return rc;
+    DGemm r;
+    r.M = naux; r.N = naux; r.K = 1;
+    r.A = c.p; r.sam = 1; r.sak = 0;
+    r.B = c.p; r.sbk = 0; r.sbn = 1;
+    r.C = W2.p; r.scm = 1; r.scn = naux;
+    r.alpha = -0.5; r.beta = 1.0;
+    if ((rc = gemm(r, "DF gradient: W2"))) return rc;
+  }
   // Y[P] = C d^P (n x o, reusing X), Z[P] = Y[P] C^T (n x n)
-  if (cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, n, o, o, &one, dC, n, 0, bt.p, o, (long long)o * o,
-                                &zero, X.p, n, (long long)n * o, naux) != CUBLAS_STATUS_SUCCESS ||
-      cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_T, n, n, o, &one, X.p, n, (long long)n * o, dC, n, 0,
-                                &zero, Z.p, n, (long long)nn, naux) != CUBLAS_STATUS_SUCCESS)
-    return cublas_fail(e, "DF gradient: Z = C d C^T");
+  {
+    DGemm g;
+    g.M = n; g.N = o; g.K = o; g.batch = naux;
+    g.A = dC; g.sam = 1; g.sak = n;
+    g.B = dd.p; g.sbk = 1; g.sbn = o; g.bsb = (long long)o * o;
+    g.C = X.p; g.scm = 1; g.scn = n; g.bsc = (long long)n * o;
+    if ((rc = gemm(g, "DF gradient: Y = C d"))) return rc;
+    DGemm z;
+    z.M = n; z.N = n; z.K = o; z.batch = naux;
+    z.A = X.p; z.sam = 1; z.sak = n; z.bsa = (long long)n * o;
+    z.B = dC; z.sbk = n; z.sbn = 1;
+    z.C = Z.p; z.scm = 1; z.scn = n; z.bsc = (long long)nn;
+    if ((rc = gemm(z, "DF gradient: Z = Y C^T"))) return rc;
+  }
   k_w3<<<(unsigned)((nn * naux + 255) / 256), 256, 0, s>>>(nn, naux, c.p, dD, Z.p);
   // primitive weights of the shifted classes
   launch_scale_K((int)e->pp_p.n, e->pp_K.p, e->pp_p.p, e->pp_a.p, K2a.p, K2b.p, s);
@@ -213,14 +270,22 @@ extern "C" int jk_grad_df(jk_engine* e, const double* Cocc, int nocc, const doub
   if (st == cudaSuccess) st = cudaMemcpyAsync(dEps.p, eps_occ, sizeof(double) * nocc, cudaMemcpyHostToDevice, s);
   if (st != cudaSuccess) return check_cuda(e, st, "jk_grad_df upload");
   // D = 2 C C^T, W = C diag(eps) C^T (src/rhfgrad.cpp:35-38)
-  const double two = 2.0, one = 1.0, zero = 0.0;
-  cublasSetStream(e->cublas, s);
-  if (cublasDgemm(e->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n, n, nocc, &two, dC.p, n, dC.p, n, &zero, dD.p, n) !=
-          CUBLAS_STATUS_SUCCESS ||
-      cublasDdgmm(e->cublas, CUBLAS_SIDE_RIGHT, n, nocc, dC.p, n, dEps.p, 1, dCe.p, n) != CUBLAS_STATUS_SUCCESS ||
-      cublasDgemm(e->cublas, CUBLAS_OP_N, CUBLAS_OP_T, n, n, nocc, &one, dCe.p, n, dC.p, n, &zero, dW.p, n) !=
-          CUBLAS_STATUS_SUCCESS)
-    return set_error(e, JK_ERR_CUDA, "jk_grad_df: densities");
+  {
+    DGemm g;
+    g.M = n; g.N = n; g.K = nocc; g.alpha = 2.0;
+    g.A = dC.p; g.sam = 1; g.sak = n;
+    g.B = dC.p; g.sbk = n; g.sbn = 1;
+    g.C = dD.p; g.scm = 1; g.scn = n;
+    st = dgemm(g, s);
+    if (st == cudaSuccess) {
+      k_scale_cols<<<(unsigned)(((size_t)n * nocc + 255) / 256), 256, 0, s>>>(n, nocc, dC.p, dEps.p, dCe.p);
+      g.alpha = 1.0;
+      g.A = dCe.p;
+      g.C = dW.p;
+      st = dgemm(g, s);
+    }
+    if (st != cudaSuccess) return check_cuda(e, st, "jk_grad_df: densities");
+  }
   int rc = grad_rhf_device(e, dD.p, dW.p, 0.0, nullptr, g1.p, s, false);
   if (rc) return rc;
   rc = grad_df_2e_device(e, dC.p, nocc, dD.p, g2.p, s);
@@ -235,3 +300,9 @@ extern "C" int jk_grad_df(jk_engine* e, const double* Cocc, int nocc, const doub
     for (int i = 0; i < 3 * na; ++i) grad2e[i] = h2[i];
   return JK_OK;
 }
+
+namespace m2 {
+int grad_df_2e_tiled(jk_engine* e, const double*, int, const double*, double*, cudaStream_t) {
+  return set_error(e, JK_ERR_STATE, "DF gradient with tiled storage: not available yet");
+}
+}  // namespace m2

@@ -47,21 +47,20 @@ struct Eri3Params {
   double* T3;             // [x][P][y]
 };
 
+// Final-basis block (P|mn) of fitting shell sP and orbital shell pair ip of
+// the class: out[(a * dims[1] + x) * dims[2] + y]; c and t are scratch of
+// NP*NM*NN doubles each, the result is one of them.
 template <int LP, int LM, int LN>
-__global__ void __launch_bounds__(64) k_eri3(const Eri3Params P) {
-  constexpr int NP = ncart(LP), NM = ncart(LM), NN = ncart(LN);
-  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
-  const int is = blockIdx.y;
-  if (ip >= P.pairs.npair || is >= P.naux_shells) return;
-  const int sP = P.aux_shells[is];
+__device__ __forceinline__ const double* eri3_block(const Eri3Params& P, int sP, int ip, double* c, double* t,
+                                                    int* dims) {
   const int m = P.pairs.sa[ip], n = P.pairs.sb[ip];
   const double Ax = P.ax[sP], Ay = P.ay[sP], Az = P.az[sP];
-  double c[NP * NM * NN];
   quartet_cart<LP, 0, LM, LN>(P.ap, P.aux_prim_off[sP], P.aux_nprim[sP], Ax, Ay, Az, Ax, Ay, Az, P.pp,
                               P.pairs.prim_off[ip], P.pairs.nprim[ip], P.ox[m], P.oy[m], P.oz[m], P.ox[n], P.oy[n],
                               P.oz[n], P.boys, c);
-  double t[NP * NM * NN];
-  int dims[3] = {NP, NM, NN};
+  dims[0] = ncart(LP);
+  dims[1] = ncart(LM);
+  dims[2] = ncart(LN);
   double* cur = c;
   double* nxt = t;
   const int pure[3] = {P.aux_pure[sP], P.obs_pure[m], P.obs_pure[n]};
@@ -74,6 +73,20 @@ __global__ void __launch_bounds__(64) k_eri3(const Eri3Params P) {
       cur = nxt;
       nxt = sw;
     }
+  return cur;
+}
+
+template <int LP, int LM, int LN>
+__global__ void __launch_bounds__(64) k_eri3(const Eri3Params P) {
+  constexpr int N3 = ncart(LP) * ncart(LM) * ncart(LN);
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  const int is = blockIdx.y;
+  if (ip >= P.pairs.npair || is >= P.naux_shells) return;
+  const int sP = P.aux_shells[is];
+  const int m = P.pairs.sa[ip], n = P.pairs.sb[ip];
+  double c[N3], t[N3];
+  int dims[3];
+  const double* cur = eri3_block<LP, LM, LN>(P, sP, ip, c, t, dims);
   const int f0 = P.aux_foff[sP], m0 = P.obs_foff[m], n0 = P.obs_foff[n];
   const size_t nQ = (size_t)P.naux * P.n;
   for (int a = 0; a < dims[0]; ++a)
@@ -82,6 +95,45 @@ __global__ void __launch_bounds__(64) k_eri3(const Eri3Params P) {
         const double v = cur[(a * dims[1] + x) * dims[2] + y];
         P.T3[(size_t)(m0 + x) * nQ + (size_t)(f0 + a) * P.n + n0 + y] = v;
         P.T3[(size_t)(n0 + y) * nQ + (size_t)(f0 + a) * P.n + m0 + x] = v;
+      }
+}
+
+// One tile pair of the tiled three-index tensor: T[r][P][c] = (P | x y) for
+// x = x0 + r and y = y0 + c inside the TB x TB tile (TB = 128), over the
+// shell pairs `plist` of the class that touch the tile pair (either
+// orientation).  Entries of the block outside the tile are not written.
+struct Eri3TileArgs {
+  const int* plist;  // indices into the class's pair list
+  int nlist;
+  int x0, y0;        // first function of the row tile and of the column tile
+  int naux;
+  double* T;         // [r][P][c], TB * naux * TB doubles
+};
+constexpr int DF_TILE = 128;
+
+template <int LP, int LM, int LN>
+__global__ void __launch_bounds__(64) k_eri3_tile(const Eri3Params P, const Eri3TileArgs A) {
+  constexpr int N3 = ncart(LP) * ncart(LM) * ncart(LN);
+  const int il = blockIdx.x * blockDim.x + threadIdx.x;
+  const int is = blockIdx.y;
+  if (il >= A.nlist || is >= P.naux_shells) return;
+  const int ip = A.plist[il];
+  const int sP = P.aux_shells[is];
+  const int m = P.pairs.sa[ip], n = P.pairs.sb[ip];
+  double c[N3], t[N3];
+  int dims[3];
+  const double* cur = eri3_block<LP, LM, LN>(P, sP, ip, c, t, dims);
+  const int f0 = P.aux_foff[sP], m0 = P.obs_foff[m], n0 = P.obs_foff[n];
+  const size_t rs = (size_t)A.naux * DF_TILE;  // stride of r
+  for (int a = 0; a < dims[0]; ++a)
+    for (int x = 0; x < dims[1]; ++x)
+      for (int y = 0; y < dims[2]; ++y) {
+        const double v = cur[(a * dims[1] + x) * dims[2] + y];
+        const int X = m0 + x, Y = n0 + y;
+        const unsigned r1 = (unsigned)(X - A.x0), c1 = (unsigned)(Y - A.y0);
+        if (r1 < DF_TILE && c1 < DF_TILE) A.T[r1 * rs + (size_t)(f0 + a) * DF_TILE + c1] = v;
+        const unsigned r2 = (unsigned)(Y - A.x0), c2 = (unsigned)(X - A.y0);
+        if (r2 < DF_TILE && c2 < DF_TILE) A.T[r2 * rs + (size_t)(f0 + a) * DF_TILE + c2] = v;
       }
 }
 
@@ -241,6 +293,10 @@ void launch_eri3_l0(int pair_class_id, const Eri3Params& P, cudaStream_t s);
 void launch_eri3_l1(int pair_class_id, const Eri3Params& P, cudaStream_t s);
 void launch_eri3_l2(int pair_class_id, const Eri3Params& P, cudaStream_t s);
 void launch_eri3_l3(int pair_class_id, const Eri3Params& P, cudaStream_t s);
+void launch_eri3_tile_l0(int pair_class_id, const Eri3Params& P, const Eri3TileArgs& A, cudaStream_t s);
+void launch_eri3_tile_l1(int pair_class_id, const Eri3Params& P, const Eri3TileArgs& A, cudaStream_t s);
+void launch_eri3_tile_l2(int pair_class_id, const Eri3Params& P, const Eri3TileArgs& A, cudaStream_t s);
+void launch_eri3_tile_l3(int pair_class_id, const Eri3Params& P, const Eri3TileArgs& A, cudaStream_t s);
 void launch_eri2(int LP, int LQ, const Eri2Params& P, cudaStream_t s);
 void launch_onebody(int pair_class_id, const OneBodyParams& P, cudaStream_t s);
 

@@ -470,7 +470,7 @@ __global__ void k_zero_upper(int n, double* J) {
 }
 
 // ---------------------------------------------------------------- host
-static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
     cudaDriverEntryPointQueryResult q;
@@ -483,7 +483,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 }
 
 // 2-D BF16 tensor map: inner extent `cols` (contiguous), `rows`, box box_cols x box_rows, 128B swizzle.
-static bool make_map(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint32_t box_cols,
+bool make_map(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint32_t box_cols,
                      uint32_t box_rows) {
   auto enc = get_encode();
   if (!enc) return false;
@@ -614,6 +614,7 @@ int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double
 }
 
 int df_mixed_error(jk_engine* e) {
+  if (e->tiled.ready) return df_tiled_error(e);
   if (!e->mixed.err.p) return JK_OK;
   int h = 0;
   cudaError_t st = cudaMemcpyAsync(&h, e->mixed.err.p, sizeof(int), cudaMemcpyDeviceToHost, e->stream);
@@ -624,6 +625,50 @@ int df_mixed_error(jk_engine* e) {
     return set_error(e, JK_ERR_CUDA, "mixed DF: tensor-core pipeline wait timed out (stage " + std::to_string(h) + ")");
   }
   return JK_OK;
+}
+
+// ---------------------------------------------------------------- shared with the tiled path
+cudaError_t launch_split_C(int n, int nocc, int NP, int ld, const double* C, __nv_bfloat16* Ch, __nv_bfloat16* Cl,
+                           cudaStream_t s) {
+  k_split_C<<<dim3((ld + 127) / 128, NP), 128, 0, s>>>(n, nocc, NP, ld, C, Ch, Cl);
+  return cudaGetLastError();
+}
+
+// Kt (+)= X X^T over the lower-triangle 128 x 128 tiles of the n rows of X
+// (tensor maps tXh, tXl over rows of `kblocks` * 64 BF16), split-K over the SMs.
+cudaError_t launch_gemm2(const CUtensorMap& tXh, const CUtensorMap& tXl, int n, int kblocks, double* Kt, int* err,
+                         int nsm, cudaStream_t s) {
+  G2Params P2{};
+  P2.n = n;
+  P2.kblocks = kblocks;
+  P2.ntile_n = (n + BM - 1) / BM;
+  P2.ntiles_u = P2.ntile_n * (P2.ntile_n + 1) / 2;
+  // splits so that the CTA count is close to a whole number of waves
+  int best = 1;
+  double best_eff = 0.0;
+  for (int sp = 1; sp <= 16 && sp <= kblocks; ++sp) {
+    const int ctas = P2.ntiles_u * sp;
+    const double waves = std::ceil((double)ctas / nsm);
+    const double eff = (double)ctas / (waves * nsm);
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = sp;
+    }
+    if (eff > 0.97) break;
+  }
+  P2.splits = best;
+  P2.Kt = Kt;
+  P2.err = err;
+  cudaError_t st = cudaFuncSetAttribute(k_gemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, G2_SMEM);
+  if (st != cudaSuccess) return st;
+  k_gemm2<<<P2.ntiles_u * P2.splits, 192, G2_SMEM, s>>>(tXh, tXl, P2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_mixed(int n, const double* Kt, double* J, double* K, cudaStream_t s) {
+  const size_t nn = (size_t)n * n;
+  k_finalize_mixed<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(n, Kt, J, K);
+  return cudaGetLastError();
 }
 
 }  // namespace m2

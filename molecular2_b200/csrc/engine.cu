@@ -394,10 +394,9 @@ int jk_schwarz(const jk_engine* e, double* Q) {
 }
 
 long long jk_last_quartets(const jk_engine* e) {
-  if (!e || !e->Dmax.p) return -1;
+  if (!e || !e->last_counter) return -1;
   unsigned long long c = 0;
-  // the direct build keeps its quartet counter in the word after Dmax
-  if (cudaMemcpyAsync(&c, e->Dmax.p + 1, sizeof(c), cudaMemcpyDeviceToHost, e->stream) != cudaSuccess) return -1;
+  if (cudaMemcpyAsync(&c, e->last_counter, sizeof(c), cudaMemcpyDeviceToHost, e->stream) != cudaSuccess) return -1;
   if (cudaStreamSynchronize(e->stream) != cudaSuccess) return -1;
   return (long long)c;
 }

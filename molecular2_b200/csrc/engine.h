@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -84,6 +85,7 @@ struct DFState {
   int k0 = 0, k1 = -1;      // fitted-index range kept in HBM (k1 < 0: all)
   DevBuf<double> B64;      // [x][K][y] unpacked, FP64
   DevBuf<double> L;        // Cholesky factor of the metric (naux x naux, col-major)
+  DevBuf<double> Linv;     // L^-1 (naux x naux, col-major, strict upper triangle zero)
   DevBuf<double> X64;      // [x][K][i]
   DevBuf<double> gamma;    // naux
 };
@@ -99,6 +101,26 @@ struct MixedState {
   DevBuf<double> Kt;                 // n x n partial K (lower-triangle tiles)
   DevBuf<int> err;                   // pipeline error word
   CUtensorMap maps[6];               // Bh, Bl, Ch, Cl, Xh, Xl
+};
+
+// Large-system DF storage: the fitted tensor B_K (symmetric in x, y) kept
+// only on and below the diagonal, in 128 x 128 function tiles, as split BF16
+// [K][tile pair][r][c]; the FP64 build streams (P|mn) tile pairs instead of
+// keeping them.
+struct TiledDF {
+  bool ready = false;                // fitted tensor built (jk_df_setup)
+  bool metric_ready = false;         // metric factor, its inverse and the tile lists
+  int nt = 0, npt = 0, npad = 0;     // tile rows, stored tile pairs, padded n
+  std::vector<long long> list_off;   // [tile pair][class] offsets into plist (+1 entry)
+  DevBuf<int> plist;                 // pair indices (into the class lists) touching each tile pair
+  DevBuf<__nv_bfloat16> Bh, Bl;      // [K][t][r][c]
+  // mixed-build scratch
+  int NPX = 0, waux = 0, nocc = 0;   // X row length per K (nhalf * 160), aux block, occupied count
+  DevBuf<__nv_bfloat16> Ch, Cl;      // [i][y], NPX x npad
+  DevBuf<__nv_bfloat16> Xh, Xl;      // [x][K_local][i], npad x waux x NPX
+  DevBuf<double> Kt;                 // n x n lower-tile K
+  DevBuf<int> err;
+  CUtensorMap maps[8];               // Bh/Bl K-major, Bh/Bl MN-major, Ch, Cl, Xh, Xl
 };
 
 }  // namespace m2
@@ -134,7 +156,11 @@ struct jk_engine {
   m2::DevBuf<double> Dcart, Jcart, Kcart, Dnorm, Dmax, Dfinal, Jfinal, Kfinal;
   m2::DFState df;
   m2::MixedState mixed;
-  long long last_quartets = 0;
+  m2::TiledDF tiled;
+  int df_storage = 0;     // jk_df_set_storage: 0 auto, 1 unpacked FP64, 2 tiled
+  // quartet counter of the last direct build (engine scratch or the fixed
+  // array of jk_direct_noalloc), read by jk_last_quartets
+  const unsigned long long* last_counter = nullptr;
   // optional per-stage CUDA-event timing of the DF build (jk_set_profiling)
   bool profiling = false;
   static constexpr int NSTAGE_EV = 8;
@@ -153,13 +179,31 @@ int build_pairs(jk_engine* e);
 int direct_jk_device(jk_engine* e, const double* dD, double precision, double mult, double* dJ, double* dK,
                      cudaStream_t s);
 // df.cu
+int prepare_aux(jk_engine* e);
+int compute_V(jk_engine* e, double* V, cudaStream_t s);
 int df_setup(jk_engine* e);
 int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ, double* dK, cudaStream_t s);
+cudaError_t df_syrk_X(jk_engine* e, const double* X, int n, long long len, double* K, cudaStream_t s);
 int one_body_device(jk_engine* e, double* S, double* T, double* V, cudaStream_t s);
 void stage_mark(jk_engine* e, int k, cudaStream_t s);
 // df_mixed.cu
 int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double* dK, cudaStream_t s);
 int df_mixed_error(jk_engine* e);
+bool make_map(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint32_t box_cols, uint32_t box_rows);
+cudaError_t launch_split_C(int n, int nocc, int NP, int ld, const double* C, __nv_bfloat16* Ch, __nv_bfloat16* Cl,
+                           cudaStream_t s);
+cudaError_t launch_gemm2(const CUtensorMap& tXh, const CUtensorMap& tXl, int n, int kblocks, double* Kt, int* err,
+                         int nsm, cudaStream_t s);
+cudaError_t launch_finalize_mixed(int n, const double* Kt, double* J, double* K, cudaStream_t s);
+// df_tiled.cu
+int df_tiled_setup(jk_engine* e);
+int df_tiled_metric(jk_engine* e);
+int tiled_xprime_pass(jk_engine* e, const double* Cp, int i0, int ocur, double* X, double* Tt, cudaStream_t s,
+                      const std::function<int(int, int, int)>& hook);
+void launch_pad_rows(int n, int npad, int nocc, const double* C, double* Cp, cudaStream_t s);
+int df_tiled_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ, double* dK, cudaStream_t s);
+bool df_use_tiled(jk_engine* e);
+int df_tiled_error(jk_engine* e);
 // transforms (cart <-> final) and norms
 void launch_final_to_cart(const jk_engine* e, const double* Dfinal, double* Dcart, cudaStream_t s);
 void launch_cart_to_final_sym(const jk_engine* e, const double* Xcart, double scale, double* Xfinal, cudaStream_t s);

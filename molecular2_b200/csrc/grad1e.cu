@@ -7,23 +7,27 @@
 
 namespace m2 {
 
-// sum_tuv E^{ab}_t E_u E_v R[t+st, u+su, v+sv] for one Cartesian pair (a, b);
-// NR is the length of R.  Kept out of line: inlined into k_grad1e, ptxas
-// (CUDA 12.9, -O1 and above) produced wrong nuclear-attraction sums for the
-// p-shell classes, while -O0 and this out-of-line form agree with a host
-// build of the same source.
+// sum_tuv E^{ab}_t E_u E_v R[t+st, u+su, v+sv] for one Cartesian pair (a, b).
+// Bound: every caller passes components with |a| + |b| + st + su + sv <=
+// LA + LB + 1 = L (the Hellmann-Feynman term: |a| = LA, |b| = LB and one unit
+// shift; the centre terms: a or b raised or lowered by one, no shift), so
+// hidx(...) < nherm(L) = NR for every term; the static_assert ties NR to the
+// class.  Kept out of line: inlined into k_grad1e, the CUDA 12.9 build at
+// ptxas -O1 and above gave wrong nuclear-attraction sums for the p-shell
+// classes, while -O0 and this out-of-line form agree with a host build of the
+// same source.  Reading the kernel found no out-of-bounds index or other
+// source defect behind it, so the out-of-line form is a workaround kept for a
+// compiler behaviour whose cause is not known.
 template <int LA1, int LB2, int NR>
 __device__ __noinline__ double herm_sum(const E1<LA1, LB2>& ex, const E1<LA1, LB2>& ey, const E1<LA1, LB2>& ez,
                                         int ax, int ay, int az, int bx, int by, int bz, const double* R, int st,
                                         int su, int sv) {
+  static_assert(NR == nherm(LA1 + LB2 - 2), "R table length must be nherm(LA + LB + 1)");
   double acc = 0.0;
   for (int t = 0; t <= ax + bx; ++t)
     for (int u = 0; u <= ay + by; ++u) {
       const double exy = ex.e[ax][bx][t] * ey.e[ay][by][u];
-      for (int v = 0; v <= az + bz; ++v) {
-        const int h = hidx(t + st, u + su, v + sv);
-        if (h < NR) acc += exy * ez.e[az][bz][v] * R[h];
-      }
+      for (int v = 0; v <= az + bz; ++v) acc += exy * ez.e[az][bz][v] * R[hidx(t + st, u + su, v + sv)];
     }
   return acc;
 }

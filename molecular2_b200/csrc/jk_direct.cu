@@ -195,6 +195,7 @@ int direct_jk_device(jk_engine* e, const double* dD, double precision, double mu
   cudaMemsetAsync(e->Jcart.p, 0, sizeof(double) * nc * nc, s);
   cudaMemsetAsync(e->Kcart.p, 0, sizeof(double) * nc * nc, s);
   unsigned long long* counter = reinterpret_cast<unsigned long long*>(e->Dmax.p + 1);
+  e->last_counter = counter;
   cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
   JKParams P{};
   P.pp = prim_view(e);
@@ -268,8 +269,17 @@ int direct_jk_noalloc(jk_engine* e, const double* dD, double precision, double m
                      "jk_direct_noalloc: basis too large for the fixed scratch (" + std::to_string(nc) +
                          " Cartesian functions, max " + std::to_string(NOALLOC_MAX_CART) + "; " + std::to_string(ns) +
                          " shells, max " + std::to_string(NOALLOC_MAX_SHELLS) + "); use jk_direct_device");
+  // the array's address is per device: launching on another GPU than the
+  // engine's would hand its kernels a foreign address
+  int cur = -1;
+  cudaError_t st = cudaGetDevice(&cur);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_direct_noalloc: cudaGetDevice");
+  if (cur != e->device)
+    return set_error(e, JK_ERR_ARG,
+                     "jk_direct_noalloc: the current CUDA device (" + std::to_string(cur) +
+                         ") is not the engine's device (" + std::to_string(e->device) + ")");
   double* base = nullptr;
-  cudaError_t st = noalloc_scratch(e->device, &base);
+  st = noalloc_scratch(e->device, &base);
   if (st != cudaSuccess) return check_cuda(e, st, "jk_direct_noalloc: cudaGetSymbolAddress");
   double* Dc = base;
   double* Jc = base + NOALLOC_CC;
@@ -277,6 +287,7 @@ int direct_jk_noalloc(jk_engine* e, const double* dD, double precision, double m
   double* Dn = base + 3 * NOALLOC_CC;
   double* Dmax = Dn + NOALLOC_SS;
   unsigned long long* counter = reinterpret_cast<unsigned long long*>(Dmax + 1);
+  e->last_counter = counter;
   // the array keeps the previous call's contents: clear the accumulators
   launch_shell_norms(e, dD, Dn, Dmax, s);  // zeroes Dmax itself
   launch_final_to_cart(e, dD, Dc, s);

@@ -120,6 +120,21 @@ __device__ __forceinline__ uint64_t sdesc_kmajor_sw128(const void* smem) {
   return d;
 }
 
+// Shared-memory matrix descriptor: MN-major, 128-byte swizzle.  Each 128 B
+// row holds 64 consecutive M (or N) elements at one k; 8 k rows form a
+// 1024 B swizzle atom.  lbo_bytes: distance between 64-element M groups;
+// sbo_bytes: distance between 8-row k groups.
+__device__ __forceinline__ uint64_t sdesc_mnmajor_sw128(const void* smem, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  const uint64_t addr = smem_u32(smem);
+  uint64_t d = 0;
+  d |= (addr & 0x3FFFFull) >> 4;                          // [0,14)  start address >> 4
+  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;      // [16,30) LBO
+  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;      // [32,46) SBO
+  d |= (uint64_t)1 << 46;                                 // [46,48) version = 1
+  d |= (uint64_t)2 << 61;                                 // [61,64) SWIZZLE_128B
+  return d;
+}
+
 // Instruction descriptor for kind::f16: BF16 x BF16 -> FP32, both K-major.
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
   return (1u << 4)                        // D format F32
@@ -128,6 +143,8 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
          | ((uint32_t)(N >> 3) << 17)     // N >> 3
          | ((uint32_t)(M >> 4) << 24);    // M >> 4
 }
+// The same with A read MN-major (transposed A).
+__host__ __device__ constexpr uint32_t idesc_bf16_f32_amn(int M, int N) { return idesc_bf16_f32(M, N) | (1u << 15); }
 
 }  // namespace tc
 }  // namespace m2

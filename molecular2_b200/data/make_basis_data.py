@@ -3,7 +3,7 @@
 Run once, in a container that has the molecular2 sources, to (re)generate
 ``basis_sets.json`` beside this file:
 
-    python molecular2_b200/data/make_basis_data.py /root/reference
+    python molecular2_b200/data/make_basis_data.py <molecular2 checkout>
 
 Basis sets are published data (EMSL Basis Set Exchange); molecular2 ships
 them in two formats and this script reads both the way molecular2 does:
@@ -104,4 +104,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of a molecular2 checkout>")
+    main(sys.argv[1])

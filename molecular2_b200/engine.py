@@ -42,6 +42,8 @@ SIGNATURES = {
     "jk_eri2": (_I, [_P, _P]),
     "jk_df_setup": (_I, [_P]),
     "jk_df_set_range": (_I, [_P, _I, _I]),
+    "jk_df_set_storage": (_I, [_P, _I]),
+    "jk_df_storage": (_I, [_P]),
     "jk_df": (_I, [_P, _P, _I, _I, _P, _P]),
     "jk_df_device": (_I, [_P, _P, _I, _I, _P, _P, _P]),
     "jk_one_body": (_I, [_P, _P, _P, _P]),
@@ -190,6 +192,19 @@ class IntegralEngine:
 
     def df_setup(self):
         self._check(self.lib.jk_df_setup(self.h))
+
+    DF_STORAGE = {"auto": 0, "unpacked": 1, "tiled": 2}
+
+    def set_df_storage(self, mode):
+        """Layout of the fitted tensor (before df_setup): "unpacked" FP64
+        B[x][K][y], "tiled" symmetric 128 x 128 tiles in split BF16 with the
+        FP64 build streaming the integrals, or "auto" (tiled when the unpacked
+        tensor would not fit on the device)."""
+        self._check(self.lib.jk_df_set_storage(self.h, self.DF_STORAGE[mode]))
+
+    @property
+    def df_storage(self):
+        return {0: None, 1: "unpacked", 2: "tiled"}[int(self.lib.jk_df_storage(self.h))]
 
     @property
     def df_range(self):

@@ -2,7 +2,7 @@
 
 Run in a container that has the molecular2 sources:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <molecular2 checkout>
 
 molecular2 has no automated tests; its only expected values are hand-run
 outputs kept in ``test/``.  This script copies the numbers out of them:
@@ -65,4 +65,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of a molecular2 checkout>")
+    main(sys.argv[1])
