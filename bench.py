@@ -1,27 +1,40 @@
 #!/usr/bin/env python
-"""Benchmark of the J/K engine on the (H2O)16 DF-JK workload.
+"""Benchmark of the J/K engine on (H2O)64 / aug-cc-pVDZ + AVDZ-JKFIT.
 
-Workload: (H2O)16 water cluster (seeded, 9 A cube), RHF/cc-pVDZ (n = 384)
-with the VDZ-JKFIT fitting basis (naux = 1856), nocc = 80: the density-fitted
-J/K build molecular2 runs every SCF iteration (Fock::formJKdf,
-src/fockbuild.cpp:171-174, 585-660).  A step is one J/K build for the
+Workload (the north-star system): 64 rigid water monomers placed by seeded
+random rotation and translation in a 14 A cube (O-O >= 2.7 A), RHF with the
+aug-cc-pVDZ orbital basis (n = 2624) and the AVDZ-JKFIT fitting basis
+(naux = 9600), nocc = 320: the density-fitted J/K build molecular2 runs every
+SCF iteration (Fock::formJKdf, src/fockbuild.cpp:171-174, 585-660).  The
+fitted tensor is kept in the tiled split-BF16 layout (145 GB); the FP64 path
+recomputes the three-index integrals per build.
+
+A step is one mixed-precision (split-BF16 tcgen05) J/K build for the
 converged occupied orbitals; `value` is builds/s with everything resident in
-HBM, `e2e` the same through the host-pointer C entry point (C uploaded, J and
-K downloaded every step).  The whole RHF SCF is timed once per precision
-mode and reported under "scf" (mixed = split-BF16 tensor-core builds, then
-FP64 builds to convergence), with |dE| between the two.  Two more
-workloads are timed once and reported beside the line: the FP64 analytic
-gradient of (H2O)8/cc-pVDZ ("gradient") and one FP64 integral-direct J/K
-build of C20H42/6-311G** ("direct_jk"); --no-extras skips them.
+HBM (inputs are larger than L2: 145 GB of B per build), `e2e` the same through
+the host-pointer entry point jk_df (C uploaded, J and K downloaded every step).
+Reported beside it, each timed once:
+  * "scf": the FP64 SCF and the mixed SCF (split-BF16 builds, one FP64
+    correction at the switch, final FP64 energy) from the SOAD guess, their
+    wall times, iterations, J/K time and |dE|;
+  * "jk_builds_per_s": mixed (the timed steps) and FP64 (from the FP64 SCF's
+    builds), and the mixed build's J/K error against an FP64 build;
+  * "gradient": one DF nuclear gradient at the mixed-SCF orbitals;
+  * "df_setup_s": metric factorisation and tiled fitted tensor;
+  * "extras": the smaller workloads ((H2O)16 DF builds, C20H42 direct build,
+    (H2O)8 FP64 and DF gradients); --no-extras skips them.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision mixed|fp64] [--profile]
+                    [--workload water64|water16] [--profile]
 
 --impl reference times molecular2's own algorithm on the host cores: the
 oracle's restatement of compute_2body_fock_df's naive loops (molecular2
-itself needs libint2/Eigen and cannot be built here), on a bounded sample of
-the fitting functions, extrapolated linearly in naux.
---profile runs only the timed builds (no SCF, e2e or CPU leg) for ncu.
+itself needs libint2/Eigen and cannot be built here; its packed FP64 B for
+this system would be 264 GB), on a bounded sample of the fitting functions,
+extrapolated linearly in naux.
+--profile runs only the set-up and the timed builds (for ncu launch lists).
+With --gpus N > 1 every rank runs its own replica of the workload (the
+north-star measurement is single-GPU).
 """
 import argparse
 import ctypes
@@ -38,42 +51,38 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "DF-JK Fock builds/s, (H2O)16 RHF/cc-pVDZ + VDZ-JKFIT"
+METRIC = "SCF time & J/K builds/s, mixed vs FP64 GPU at |dE|<=1e-6 Eh; gradient time"
 UNIT = "builds/s"
-SEED = 16
+WORKLOADS = {
+    "water64": dict(label="(H2O)64 RHF/aug-cc-pVDZ + AVDZ-JKFIT", k=64, box=14.0, seed=64,
+                    obs="aug-cc-pvdz", aux="avdz-jkfit", storage="tiled"),
+    "water16": dict(label="(H2O)16 RHF/cc-pVDZ + VDZ-JKFIT", k=16, box=9.0, seed=16,
+                    obs="cc-pvdz", aux="vdz-jkfit", storage="unpacked"),
+}
+_CACHE = {}
 
 
-_WORKLOAD = None
-
-
-def workload():
-    global _WORKLOAD
-    if _WORKLOAD is None:
+def workload(name):
+    if name not in _CACHE:
         from molecular2_b200 import geometry
         from molecular2_b200.basis import BasisSet
-        mol = geometry.water16(SEED)
-        _WORKLOAD = (mol, BasisSet(mol, "cc-pvdz"), BasisSet(mol, "vdz-jkfit"))
-    return _WORKLOAD
+        w = WORKLOADS[name]
+        mol = geometry.water_cluster(w["k"], w["box"], w["seed"])
+        _CACHE[name] = (mol, BasisSet(mol, w["obs"]), BasisSet(mol, w["aux"]))
+    return _CACHE[name]
 
 
-def traffic(kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu capture (None if absent)."""
-    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if not os.path.exists(p):
-        return None
-    k = json.load(open(p)).get("kernels", {}).get(kernel)
-    return k["dram_bytes_read"] + k["dram_bytes_write"] if k else None
-
-
-def config(mol, obs, aux, prec, world=1):
-    return {"workload": f"(H2O)16 RHF/cc-pVDZ + VDZ-JKFIT DF-JK build (n={obs.nbf}, naux={aux.nbf}, "
-                        f"nocc={mol.nocc}), seed {SEED}",
-            "precision": prec,
-            "l2": "inputs larger than L2 (B tensor %.2f GB FP64 / %.2f GB split BF16)"
-                  % (obs.nbf ** 2 * aux.nbf * 8 / 1e9, obs.nbf ** 2 * aux.nbf * 4 / 1e9),
-            "parallelism": ("single GPU" if world == 1 else
-                            f"aux-sharded x{world}: fitted-index slices per rank, one NCCL all-reduce of J and K "
-                            "per build")}
+def config(name, mol, obs, aux, world=1):
+    w = WORKLOADS[name]
+    gb = obs.nbf * obs.nbf * aux.nbf
+    return {"workload": f"{w['label']} DF-JK build (n={obs.nbf}, naux={aux.nbf}, nocc={mol.nocc}), "
+                        f"{w['k']} waters in a {w['box']:.0f} A cube, seed {w['seed']}",
+            "precision": "mixed split-BF16 (hi*hi + hi*lo + lo*hi, FP32 accumulate) build; FP64 SCF and "
+                         "corrections",
+            "storage": w["storage"],
+            "l2": "inputs larger than L2 (fitted tensor %.1f GB split BF16 per build)"
+                  % ((gb / 2 if w["storage"] == "tiled" else gb) * 4 / 1e9),
+            "parallelism": "single GPU" if world == 1 else f"{world} independent replicas, one per GPU"}
 
 
 def peaks():
@@ -84,32 +93,33 @@ def peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+def traffic(kernel):
+    """DRAM bytes per launch of `kernel` at the benchmark size, from the committed ncu summary (None if absent)."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    k = json.load(open(p)).get("kernels", {}).get(kernel)
+    return k.get("dram_bytes_per_launch_full_size") if k else None
+
+
 # ---------------------------------------------------------------- CPU leg
-def cpu_sample(nthreads, target_s=12.0):
-    """Time the naive per-iteration loops of compute_2body_fock_df on a
-    contiguous block of fitting functions, doubling the block until one run
-    takes target_s / 3 (the whole sample stays within about target_s);
-    returns (builds/s extrapolated to all fitting functions, sample text, s)."""
+def cpu_sample(name, nthreads, target_s=12.0):
+    """Time the naive per-iteration loops of compute_2body_fock_df (the
+    oracle's restatement) on a block of fitting functions of workload `name`,
+    doubling the block until one run takes target_s / 3; returns (builds/s
+    extrapolated to all fitting functions, sample text, seconds spent)."""
     import oracle
-    mol, obs, aux = workload()
+    mol, obs, aux = workload(name)
     n, naux, nocc = obs.nbf, aux.nbf, mol.nocc
     rng = np.random.default_rng(0)
     npair = n * (n + 1) // 2
     C = np.asfortranarray(rng.normal(size=(n, nocc)))
-    Bfull = None
-
-    def run(nk):
-        B = np.asfortranarray(Bfull[:, :nk])
+    nk, prev, total = 1, None, 0.0
+    while True:
+        B = np.asfortranarray(rng.normal(size=(npair, nk)))
         t = time.perf_counter()
         oracle.df_jk(B, C, (0, nk), nthreads=nthreads)
-        return time.perf_counter() - t
-
-    nk, prev, total = 2, None, 0.0
-    Bfull = np.asfortranarray(rng.normal(size=(npair, 2)))
-    while True:
-        if Bfull.shape[1] < nk:
-            Bfull = np.asfortranarray(rng.normal(size=(npair, nk)))
-        t = run(nk)
+        t = time.perf_counter() - t
         total += t
         if t >= target_s / 3 or nk >= naux:
             break
@@ -121,8 +131,8 @@ def cpu_sample(nthreads, target_s=12.0):
     else:
         t_full = t * naux / nk
     sample = (f"naive X/K/gamma/J loops of compute_2body_fock_df over {nk} of {naux} fitting functions "
-              f"(synthetic B values), {nthreads} thread(s), last run {t:.2f} s of {total:.1f} s sampled, "
-              f"extrapolated linearly to {naux}")
+              f"(synthetic B values, n={n}, nocc={nocc}), {nthreads} thread(s), last run {t:.2f} s of "
+              f"{total:.1f} s sampled, extrapolated linearly to {naux}")
     return 1.0 / t_full, sample, total
 
 
@@ -130,22 +140,22 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     nthreads = os.cpu_count() or 1
-    # each step a bounded sample, sized so that warm-up + steps take about 2-3 minutes
-    per_step = min(3.0, max(0.3, 150.0 / max(1, args.steps + args.warmup)))
+    per_step = min(6.0, max(0.5, 150.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
-        cpu_sample(nthreads, target_s=per_step)
+        cpu_sample(args.workload, nthreads, target_s=per_step)
     vals = []
     t0 = time.perf_counter()
     sample = ""
     for _ in range(args.steps):
-        v, sample, _ = cpu_sample(nthreads, target_s=per_step)
+        v, sample, _ = cpu_sample(args.workload, nthreads, target_s=per_step)
         vals.append(v)
     wall = time.perf_counter() - t0
     v = statistics.median(vals)
-    mol, obs, aux = workload()
+    mol, obs, aux = workload(args.workload)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(mol, obs, aux, "fp64"),
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config(args.workload, mol, obs, aux),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
@@ -193,64 +203,56 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def roofline_fp64(n, naux, nocc, stages):
-    names = ["X=B.C (cuBLAS DGEMM)", "K=X.X^T (cuBLAS DGEMM)", "gamma (k_gamma)", "J=B.gamma (k_df_J_lower)"]
+# ---------------------------------------------------------------- roofline
+def roofline_tiled(n, naux, nocc, st):
+    """Tiled mixed build.  st = [GEMM1 total ms, GEMM2 total ms, J ms,
+    finalize ms, blocks].  Algorithmic work (B counted unpacked): GEMM1
+    X = B C is 2 n^2 o naux flops, GEMM2 K = X X^T n(n+1) o naux flops; J
+    reads the stored tiles (split BF16) once."""
     hbm, bf16, src = peaks()
-    B_bytes = (n * (n + 1) // 2) * naux * 8   # k_df_J_lower reads the lower half of B
-    own = 3
-    ach = B_bytes / (stages[own] * 1e-3) / 1e9 if len(stages) > own else None
-    return {"kernel": names[own], "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-            "frac": ach / hbm if ach else None, "traffic": None, "peak_source": src,
-            "algorithmic_bytes_per_launch": B_bytes,
-            "stage_ms": {names[i]: round(float(stages[i]), 5) for i in range(len(stages))}}
+    nt = (n + 127) // 128
+    g1_flops = 2.0 * n * n * nocc * naux
+    g2_flops = 1.0 * n * (n + 1) * nocc * naux
+    j_bytes = naux * (nt * (nt + 1) // 2) * 128 * 128 * 4.0
+    nhalf = (nocc + 159) // 160
+    g1_exec = 3 * 2.0 * (nt * 128) ** 2 * (nhalf * 160) * naux      # split products over padded tiles
+    g1, g2, jm, fm, blocks = st[:5]
+    blocks = max(1, int(round(blocks)))
+    stages = [{"kernel": "k_gemm1_sym (X = B C, tcgen05, symmetric tiles)", "ms_total": g1, "launches": blocks,
+               "ms_per_launch": g1 / blocks, "bound": "tensor", "algorithmic_tflops": g1_flops / g1 / 1e9,
+               "frac_of_bf16_peak": g1_flops / g1 / 1e9 / bf16,
+               "executed_tflops": g1_exec / g1 / 1e9, "frac_executed": g1_exec / g1 / 1e9 / bf16},
+              {"kernel": "k_gemm2 (K = X X^T, tcgen05)", "ms_total": g2, "launches": blocks, "bound": "tensor",
+               "algorithmic_tflops": g2_flops / g2 / 1e9, "frac_of_bf16_peak": g2_flops / g2 / 1e9 / bf16},
+              {"kernel": "k_J_tiles (J = sum_K gamma_K B_K)", "ms": jm, "bound": "hbm",
+               "achieved_GBs": j_bytes / jm / 1e6, "frac_of_hbm": j_bytes / jm / 1e6 / hbm},
+              {"kernel": "k_finalize_mixed", "ms": fm}]
+    ach = g1_flops / g1 / 1e9
+    return {"kernel": "k_gemm1_sym", "bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
+            "frac": ach / bf16, "traffic": traffic("k_gemm1_sym"),
+            "algorithmic_flops_per_launch": g1_flops / blocks,
+            "work_model": "2 n^2 nocc w flops per launch of w fitted functions (B counted unpacked); the three "
+                          "split-BF16 products and tile padding are overhead (executed_tflops)",
+            "peak_source": src, "timing": "CUDA events on the launch stream around every launch, averaged "
+                                          "over profiled steps", "stages": stages}
 
 
-def roofline_mixed(n, naux, nocc, stages):
-    """Dominant kernel of the mixed build and the per-stage bounds.
-    GEMM1 (k_gemm1): reads Bhi+Blo, writes Xhi+Xlo -> HBM-bound;
-    GEMM2 (k_gemm2): 3 split products over the lower-triangle tiles -> tensor;
-    J (k_J_mixed): reads the lower half of Bhi+Blo -> HBM-bound."""
+def roofline_unpacked(n, naux, nocc, st):
+    """Unpacked mixed build: st = [GEMM1, GEMM2, J, finalize] ms."""
     hbm, bf16, src = peaks()
     ldb = ((n + 63) // 64) * 64
     NP = ((nocc + 15) // 16) * 16
-    nt = (n + 127) // 128
-    b_bytes = 2 * n * naux * ldb * 2
-    x_bytes = 2 * n * naux * NP * 2
-    g1_bytes = b_bytes + x_bytes
-    g1_flops = 3 * 2 * (n * naux) * NP * ldb
-    g2_flops = 3 * 2 * (128 * 128) * (naux * NP) * (nt * (nt + 1) // 2)
-    j_bytes = b_bytes * (n + 1) / (2 * n)
-    names = ["split C + GEMM1 X=B.C (k_gemm1, tcgen05)", "GEMM2 K=X.X^T (k_gemm2, tcgen05)",
-             "J=B.gamma (k_J_mixed)", "finalize (k_finalize_mixed)"]
-    per = []
-    if len(stages) >= 3:
-        per = [{"stage": names[0], "ms": stages[0], "bound": "hbm", "achieved_GBs": g1_bytes / stages[0] / 1e6,
-                "frac_hbm": g1_bytes / stages[0] / 1e6 / hbm, "tflops": g1_flops / stages[0] / 1e9},
-               {"stage": names[1], "ms": stages[1], "bound": "tensor", "tflops": g2_flops / stages[1] / 1e9,
-                "frac_tensor": g2_flops / stages[1] / 1e9 / bf16},
-               {"stage": names[2], "ms": stages[2], "bound": "hbm", "achieved_GBs": j_bytes / stages[2] / 1e6,
-                "frac_hbm": j_bytes / stages[2] / 1e6 / hbm}]
-    dom = int(np.argmax(stages[:3])) if len(stages) >= 3 else 0
-    if dom == 1:
-        ach = g2_flops / stages[1] / 1e9
-        rl = {"kernel": names[1], "bound": "tensor", "achieved": ach, "peak": bf16, "unit": "TFLOP/s",
-              "frac": ach / bf16, "algorithmic_flops_per_launch": g2_flops}
-    else:
-        byts = g1_bytes if dom == 0 else j_bytes
-        ach = byts / stages[dom] / 1e6 if stages else None
-        rl = {"kernel": names[dom], "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-              "frac": ach / hbm if ach else None, "algorithmic_bytes_per_launch": byts}
-    kern = "k_gemm2" if dom == 1 else ("k_gemm1" if dom == 0 else "k_J_mixed")
-    rl.update({"traffic": traffic(kern), "traffic_source": "profiles/ncu_traffic.json (ncu dram bytes per launch)",
-               "peak_source": src, "stages": per,
-               "stage_ms": {names[i]: round(float(stages[i]), 5) for i in range(len(stages))}})
-    return rl
+    g1_bytes = 2 * n * naux * ldb * 2 + 2 * n * naux * NP * 2
+    ach = g1_bytes / st[0] / 1e6
+    return {"kernel": "k_gemm1", "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+            "traffic": None, "peak_source": src, "algorithmic_bytes_per_launch": g1_bytes,
+            "stages_ms": {"gemm1": st[0], "gemm2": st[1], "J": st[2], "finalize": st[3]}}
 
 
 # ---------------------------------------------------------------- other workloads
 def measure_gradient(local):
-    """RHF analytic gradient of (H2O)8/cc-pVDZ (n=192), FP64, after a direct
-    SCF from the SOAD guess: Fock::compute_forces (src/rhfgrad.cpp:15-89)."""
+    """RHF analytic gradient of (H2O)8/cc-pVDZ (n=192): FP64 direct
+    (Fock::compute_forces, src/rhfgrad.cpp:15-89) and DF."""
     from molecular2_b200 import geometry
     from molecular2_b200.basis import BasisSet
     from molecular2_b200.engine import IntegralEngine
@@ -263,43 +265,25 @@ def measure_gradient(local):
     C = ex["C"][:, :mol.nocc]
     W = C @ np.diag(ex["eps"][:mol.nocc]) @ C.T
     eng.compute_forces(ex["D"], W)
-    ts = []
-    for _ in range(3):
-        t = time.perf_counter()
-        g, _ = eng.compute_forces(ex["D"], W)
-        ts.append(time.perf_counter() - t)
+    t = time.perf_counter()
+    g, _ = eng.compute_forces(ex["D"], W)
+    gms = 1e3 * (time.perf_counter() - t)
     eng.close()
     out = {"workload": f"(H2O)8 RHF/cc-pVDZ analytic nuclear gradient, FP64 direct (n=192, {mol.natom} atoms), "
                        "seed 8, SOAD guess",
-           "scf_s": scf_s, "scf_iterations": r.iterations, "energy": r.energy,
-           "gradient_ms": 1e3 * statistics.median(ts), "timing": "host wall clock around jk_grad_rhf",
-           "max_abs_sum_g": float(np.abs(g.sum(axis=0)).max())}
-    # the same molecule with VDZ-JKFIT: mixed-precision DF SCF, then the DF gradient
+           "scf_s": scf_s, "scf_iterations": r.iterations, "energy": r.energy, "gradient_ms": gms,
+           "timing": "host wall clock around jk_grad_rhf", "max_abs_sum_g": float(np.abs(g.sum(axis=0)).max())}
     eng = IntegralEngine(BasisSet(mol, "cc-pvdz"), BasisSet(mol, "vdz-jkfit"), device=local)
     eng.df_setup()
-    kw = dict(df=True, guess="soad", want=True, densconverge=1e-8, enconverge=1e-10, maxiter=60)
-    eng.scf_rhf(mol.nocc, mol.enuc(), df=True, maxiter=2)
-    eng.scf_rhf(mol.nocc, mol.enuc(), df=True, prec_mode=1, maxiter=2)   # split B once, untimed
-    t = time.perf_counter()
-    r64, _ = eng.scf_rhf(mol.nocc, mol.enuc(), **kw)
-    s64 = time.perf_counter() - t
-    t = time.perf_counter()
-    rmx, ex = eng.scf_rhf(mol.nocc, mol.enuc(), prec_mode=1, **kw)
-    smx = time.perf_counter() - t
+    _, ex = eng.scf_rhf(mol.nocc, mol.enuc(), df=True, guess="soad", want=True, densconverge=1e-8,
+                        enconverge=1e-10, maxiter=60)
     o = mol.nocc
     eng.compute_forces_df(ex["C"][:, :o], ex["eps"][:o])
-    ts = []
-    for _ in range(3):
-        t = time.perf_counter()
-        gdf, _ = eng.compute_forces_df(ex["C"][:, :o], ex["eps"][:o])
-        ts.append(time.perf_counter() - t)
-    eng.close()
-    out["df"] = {"workload": "(H2O)8 RHF/cc-pVDZ + VDZ-JKFIT (naux=928): DF SCF fp64 and mixed, DF gradient at the "
-                             "mixed-SCF orbitals",
-                 "scf_fp64_s": s64, "scf_mixed_s": smx, "iterations_fp64": r64.iterations,
-                 "iterations_mixed": rmx.iterations, "abs_dE_mixed_vs_fp64": abs(rmx.energy - r64.energy),
-                 "gradient_ms": 1e3 * statistics.median(ts), "timing": "host wall clock around jk_grad_df",
+    t = time.perf_counter()
+    gdf, _ = eng.compute_forces_df(ex["C"][:, :o], ex["eps"][:o])
+    out["df"] = {"gradient_ms": 1e3 * (time.perf_counter() - t), "timing": "host wall clock around jk_grad_df",
                  "max_abs_df_minus_direct_gradient": float(np.abs(gdf - g).max())}
+    eng.close()
     return out
 
 
@@ -343,73 +327,99 @@ def measure_direct(local):
             "ms_per_build": ms, "quartets": q, "quartets_per_s": q / (ms * 1e-3)}
 
 
-def profile_direct(local):
-    """Two FP64 direct J/K builds of (H2O)8/cc-pVDZ at the density of one
-    diagonalisation of the SOAD Fock matrix (the ncu workload of the direct
-    classes)."""
-    import scipy.linalg as sl
-    from molecular2_b200 import geometry
-    from molecular2_b200.basis import BasisSet
+def measure_water16(local):
+    """(H2O)16 / cc-pVDZ + VDZ-JKFIT (unpacked storage): mixed and FP64 DF
+    build times and SCF times."""
+    import torch
     from molecular2_b200.engine import IntegralEngine
-    mol = geometry.water8()
-    eng = IntegralEngine(BasisSet(mol, "cc-pvdz"), device=local)
-    S, _, _ = eng.one_body()
-    _, C = sl.eigh(eng.soad_fock(), S)
-    D = 2.0 * C[:, :mol.nocc] @ C[:, :mol.nocc].T
-    for _ in range(2):
-        t = time.perf_counter()
-        eng.jk_direct(D, 1e-12)
-        print(json.dumps({"profile_direct": True, "build_s": time.perf_counter() - t,
-                          "quartets": eng.last_quartets()}), flush=True)
+    mol, obs, aux = workload("water16")
+    n, o = obs.nbf, mol.nocc
+    eng = IntegralEngine(obs, aux, device=local)
+    eng.set_df_storage("unpacked")
+    eng.df_setup()
+    kw = dict(df=True, densconverge=1e-6, enconverge=1e-8, guess="soad")
+    eng.scf_rhf(o, mol.enuc(), df=True, maxiter=2)
+    eng.scf_rhf(o, mol.enuc(), df=True, prec_mode=1, maxiter=2)
+    t = time.perf_counter()
+    r64, ex = eng.scf_rhf(o, mol.enuc(), want=True, **kw)
+    s64 = time.perf_counter() - t
+    t = time.perf_counter()
+    rmx, _ = eng.scf_rhf(o, mol.enuc(), prec_mode=1, mixed_refresh=1000, **kw)
+    smx = time.perf_counter() - t
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        dC = torch.from_numpy(np.ascontiguousarray(ex["C"][:, :o].T)).cuda()
+        dJ = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        dK = torch.empty_like(dJ)
+    torch.cuda.synchronize()
+    out = {"workload": f"(H2O)16 RHF/cc-pVDZ + VDZ-JKFIT (n={n}, naux={aux.nbf}), unpacked storage, SOAD guess",
+           "scf_fp64_s": s64, "scf_mixed_s": smx, "iterations_fp64": r64.iterations,
+           "iterations_mixed": rmx.iterations, "abs_dE_mixed_vs_fp64": abs(rmx.energy - r64.energy)}
+    for mode, name in ((0, "fp64"), (1, "mixed")):
+        for _ in range(3):
+            eng.jk_df_device(dC.data_ptr(), o, dJ.data_ptr(), dK.data_ptr(), mode, stream=stream.cuda_stream)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(20):
+            eng.jk_df_device(dC.data_ptr(), o, dJ.data_ptr(), dK.data_ptr(), mode, stream=stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        out[f"{name}_ms_per_build"] = ev0.elapsed_time(ev1) / 20
     eng.close()
+    return out
 
 
 # ---------------------------------------------------------------- GPU leg
 def run_ours(args, rank, world, local):
     import torch
-    import torch.distributed as dist
     from molecular2_b200.engine import IntegralEngine
     torch.cuda.set_device(local)
-    mol, obs, aux = workload()
+    name = args.workload
+    mol, obs, aux = workload(name)
     n, naux, nocc = obs.nbf, aux.nbf, mol.nocc
     eng = IntegralEngine(obs, aux, device=local)
-    t = time.perf_counter()
-    eng.df_setup()
-    setup_s = time.perf_counter() - t
-    prec_mode = {"fp64": 0, "mixed": 1}[args.precision]
-    scf = {}
+    eng.set_df_storage(WORKLOADS[name]["storage"])
+    scf, extra, fp64_build_ms = {}, {}, None
+    conv = dict(densconverge=1e-5, enconverge=1e-8, maxiter=60)
     if args.profile:
         rng = np.random.default_rng(0)
         C, _ = np.linalg.qr(rng.normal(size=(n, nocc)))
+        t = time.perf_counter()
+        eng.df_setup()
+        setup_s = time.perf_counter() - t
     else:
-        # SCF in both modes (not part of the timed builds); the FP64 orbitals feed the builds.
-        # One short untimed SCF first, so neither timed run pays the library's first-call setup.
-        eng.scf_rhf(nocc, mol.enuc(), df=True, maxiter=2)
-        eng.scf_rhf(nocc, mol.enuc(), df=True, prec_mode=1, maxiter=2)
         t = time.perf_counter()
-        r64, ex = eng.scf_rhf(nocc, mol.enuc(), df=True, densconverge=1e-6, enconverge=1e-8, want=True)
+        Fs = eng.soad_fock(1e-12)
+        soad_s = time.perf_counter() - t
+        # FP64 SCF first: on tiled storage it needs only the metric (the
+        # three-index integrals are recomputed per build)
+        t = time.perf_counter()
+        r64, ex = eng.scf_rhf(nocc, mol.enuc(), df=True, prec_mode=0, guess_fock=Fs, want=True, **conv)
         s64 = time.perf_counter() - t
+        fp64_build_ms = r64.jk_ms / max(1, r64.jk_builds)
         t = time.perf_counter()
-        rmx, _ = eng.scf_rhf(nocc, mol.enuc(), df=True, prec_mode=1, densconverge=1e-6, enconverge=1e-8)
+        eng.df_setup()
+        setup_s = time.perf_counter() - t
+        t = time.perf_counter()
+        rmx, exm = eng.scf_rhf(nocc, mol.enuc(), df=True, prec_mode=1, mixed_refresh=1000, guess_fock=Fs,
+                               want=True, **conv)
         smx = time.perf_counter() - t
         scf = {"fp64": {"energy": r64.energy, "iterations": r64.iterations, "converged": r64.converged,
-                        "time_s": s64, "jk_ms_total": r64.jk_ms},
+                        "time_s": s64, "jk_ms_total": r64.jk_ms, "jk_builds": r64.jk_builds,
+                        "diag_ms_total": r64.diag_ms},
                "mixed": {"energy": rmx.energy, "iterations": rmx.iterations, "converged": rmx.converged,
-                         "time_s": smx, "jk_ms_total": rmx.jk_ms, "mixed_builds": rmx.mixed_builds},
+                         "time_s": smx, "jk_ms_total": rmx.jk_ms, "jk_builds": rmx.jk_builds,
+                         "mixed_builds": rmx.mixed_builds, "fp64_builds": rmx.jk_builds - rmx.mixed_builds,
+                         "diag_ms_total": rmx.diag_ms},
                "abs_dE_mixed_vs_fp64": abs(rmx.energy - r64.energy),
                "speedup_time": s64 / smx if smx > 0 else None,
-               "convergence": "||dD||_F < 1e-6 and |dE| < 1e-8 Eh, core-Hamiltonian guess"}
+               "guess": f"SOAD ({soad_s:.1f} s, not in either SCF time)",
+               "convergence": "||dD||_F < 1e-5 and |dE| < 1e-8 Eh",
+               "mixed_schedule": "split-BF16 builds until ||dD|| < 1e-3 (or stalls), one FP64 build there for the "
+                                 "correction G64 - Gmixed, corrected mixed builds to convergence, energy from a "
+                                 "final FP64 build"}
         C = np.ascontiguousarray(ex["C"][:, :nocc])
-    if world > 1:
-        # aux-sharded build: this rank keeps only its slice of the fitted index
-        from molecular2_b200.sharding import aux_ranges
-        eng.close()
-        eng = IntegralEngine(obs, aux, device=local)
-        eng.set_df_range(*aux_ranges(naux, world)[rank])
-        t = time.perf_counter()
-        if eng.df_range[0] < eng.df_range[1]:
-            eng.df_setup()
-        setup_s = time.perf_counter() - t
+        Cm, epsm = exm["C"][:, :nocc], exm["eps"][:nocc]
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
     with torch.cuda.stream(stream):
@@ -419,17 +429,11 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
 
     def step():
-        if world > 1:
-            from molecular2_b200.sharding import df_jk_sharded
-            df_jk_sharded(eng, dC, nocc, dJ, dK, prec_mode, stream=stream)
-        else:
-            eng.jk_df_device(dC.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), prec_mode, stream=sh)
+        eng.jk_df_device(dC.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), 1, stream=sh)
 
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
     clocks = None
     if rank == 0 and not args.profile:
         clocks = Clocks(local, os.path.join(args.clock_dir or tempfile.gettempdir(), f"clocks_rank{rank}.csv"))
@@ -440,43 +444,44 @@ def run_ours(args, rank, world, local):
     ev1.record(stream)
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
-    if world > 1:
+    clk = clocks.stop() if clocks else None
+    if world > 1:   # independent replicas: the slowest rank's time, all ranks' builds
+        import torch.distributed as dist
         tt = torch.tensor([ms], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
-        dist.barrier()
-    clk = clocks.stop() if clocks else None
-    # N = 1: builds/s of one GPU; N > 1: each step is one build of the whole job
-    value = args.steps / (ms / 1e3)
+    value = world * args.steps / (ms / 1e3)
     if args.profile:
         if rank == 0:
-            print(json.dumps({"profile": True, "ms_per_step": ms / args.steps, "value": value}), flush=True)
+            print(json.dumps({"profile": True, "ms_per_step": ms / args.steps, "value": value,
+                              "df_setup_s": setup_s}), flush=True)
         eng.close()
         return
 
-    # per-stage durations of the same builds (events recorded by the library on `stream`)
+    # per-kernel durations of the same builds (events recorded by the library on `stream`)
     eng.set_profiling(True)
     acc = None
-    for _ in range(args.steps):
+    nprof = max(3, min(args.steps, 5))
+    for _ in range(nprof):
         step()
-        s = np.array(eng.stage_ms()) if eng.df_range[0] < eng.df_range[1] else np.zeros(4)
+        s = np.array(eng.stage_ms(8), dtype=float)
         acc = s if acc is None else acc + s
     eng.set_profiling(False)
-    stages = list(acc / args.steps)
-    roofline = roofline_mixed(n, naux, nocc, stages) if prec_mode == 1 else roofline_fp64(n, naux, nocc, stages)
-    if prec_mode == 1:
-        J64 = torch.empty_like(dJ)
-        K64 = torch.empty_like(dK)
-        if world > 1:
-            from molecular2_b200.sharding import df_jk_sharded
-            df_jk_sharded(eng, dC, nocc, J64, K64, 0, stream=stream)
-        else:
-            eng.jk_df_device(dC.data_ptr(), nocc, J64.data_ptr(), K64.data_ptr(), 0, stream=sh)
-        step()
-        torch.cuda.synchronize()
-        roofline["max_rel_err_vs_fp64"] = {
-            "J": float((dJ - J64).abs().max() / J64.abs().max()),
-            "K": float((dK - K64).abs().max() / K64.abs().max())}
+    st = list(acc / nprof)
+    tiled = eng.df_storage == "tiled"
+    roofline = roofline_tiled(n, naux, nocc, st) if tiled else roofline_unpacked(n, naux, nocc, st)
+    # mixed J/K error against an FP64 build at the same orbitals
+    Jm, Km = dJ.clone(), dK.clone()
+    t = time.perf_counter()
+    eng.jk_df_device(dC.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), 0, stream=sh)
+    torch.cuda.synchronize()
+    fp64_with_b_s = time.perf_counter() - t
+    err = {"J": float((Jm - dJ).abs().max() / dJ.abs().max()), "K": float((Km - dK).abs().max() / dK.abs().max()),
+           "definition": "max |mixed - FP64| over the largest |FP64| element, at the FP64-SCF orbitals"}
+    jk_rates = {"mixed": value / world, "fp64": 1e3 / fp64_build_ms if fp64_build_ms else None,
+                "fp64_source": "mean J/K build time of the FP64 SCF (metric-only storage, one integral pass per "
+                               "occupied slice plus the J pass)",
+                "fp64_build_with_tiled_B_resident_s": fp64_with_b_s, "mixed_vs_fp64_rel_err": err}
 
     # e2e: host C in (pinned), host J/K out, through the public host-pointer call
     hC = torch.from_numpy(np.asfortranarray(C)).pin_memory()
@@ -484,71 +489,69 @@ def run_ours(args, rank, world, local):
     hK = torch.empty((n, n), dtype=torch.float64).pin_memory()
 
     def e2e_step():
-        if world > 1:   # host C in, sharded build + all-reduce, host J/K out
-            with torch.cuda.stream(stream):
-                dC.copy_(hC.t(), non_blocking=True)
-            step()
-            with torch.cuda.stream(stream):
-                hJ.copy_(dJ, non_blocking=True)
-                hK.copy_(dK, non_blocking=True)
-            stream.synchronize()
-            return
-        rc = eng.lib.jk_df(eng.h, ctypes.c_void_p(hC.data_ptr()), nocc, prec_mode, ctypes.c_void_p(hJ.data_ptr()),
+        rc = eng.lib.jk_df(eng.h, ctypes.c_void_p(hC.data_ptr()), nocc, 1, ctypes.c_void_p(hJ.data_ptr()),
                            ctypes.c_void_p(hK.data_ptr()))
         if rc:
             eng._check(rc)
 
-    for _ in range(3):
+    for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
     t = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
     e2e_s = time.perf_counter() - t
-    if world > 1:
-        tt = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e = {"value": args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * nocc * 8,
-           "d2h_bytes_per_step": 2 * n * n * 8, "timing": "host wall clock around synchronous calls"}
+    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * nocc * 8,
+           "d2h_bytes_per_step": 2 * n * n * 8, "timing": "host wall clock around synchronous jk_df calls"}
+    eng.close()
 
-    other = {}
-    if rank == 0 and not args.no_extras:
-        other["gradient"] = measure_gradient(local)
-        other["direct_jk"] = measure_direct(local)
+    # one DF nuclear gradient at the mixed-SCF orbitals (fresh engine: metric only)
+    gradient = None
+    if rank == 0:
+        eng2 = IntegralEngine(obs, aux, device=local)
+        eng2.set_df_storage(WORKLOADS[name]["storage"])
+        t = time.perf_counter()
+        g, g2 = eng2.compute_forces_df(Cm, epsm)
+        gs = time.perf_counter() - t
+        eng2.close()
+        gradient = {"time_s": gs, "timing": "host wall clock around jk_grad_df (includes the metric "
+                                            "factorisation of the fresh engine)",
+                    "max_abs_sum_g": float(np.abs(g.sum(axis=0)).max()),
+                    "max_abs_g": float(np.abs(g).max()), "kind": "DF (AVDZ-JKFIT) RHF nuclear gradient, FP64"}
+        if not args.no_extras:
+            extra["water16"] = measure_water16(local)
+            extra["gradient_water8"] = measure_gradient(local)
+            extra["direct_jk_c20h42"] = measure_direct(local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, sample, _ = cpu_sample(1)
+        v, sample, _ = cpu_sample(name, 1)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
 
     if rank == 0:
-        launches = 5 if prec_mode == 1 else 3
+        blocks = int(round(st[4])) if tiled else 1
+        launches = 2 * blocks + 3   # GEMM1 and GEMM2 per block, split C, J, finalize
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak" if world == 1 else "strong", "vs_baseline": None,
-                "dtype": "f64" if prec_mode == 0 else "bf16x3->f32",
+                "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3->f32",
                 "data": "synthetic (seeded geometry; basis data from molecular2's library)",
-                "config": config(mol, obs, aux, args.precision, world), "e2e": e2e, "roofline": roofline,
+                "config": config(name, mol, obs, aux, world), "e2e": e2e, "roofline": roofline,
                 "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches * args.steps, "scf": scf,
-                "df_setup_s": setup_s, **other}
+                "jk_builds_per_s": jk_rates, "gradient": gradient, "df_setup_s": setup_s, "extras": extra}
         print(json.dumps(line), flush=True)
-    eng.close()
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="water64", choices=sorted(WORKLOADS))
     ap.add_argument("--profile", action="store_true")
     ap.add_argument("--clock-dir", default=None, help="where the nvidia-smi clock samples go (default: a temp dir)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the gradient and direct J/K measurements")
-    ap.add_argument("--profile-direct", action="store_true",
-                    help="only two FP64 direct J/K builds of (H2O)8/cc-pVDZ at the SOAD-guess density (for ncu)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the smaller workloads")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -556,15 +559,12 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.profile_direct:
-        profile_direct(local)
-        return
     if world > 1:
         import datetime
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
         run_ours(args, rank, world, local)
     finally:

@@ -142,6 +142,12 @@ int jk_df_set_range(jk_engine* e, int k0, int k1);
 int jk_df_set_storage(jk_engine* e, int mode);
 int jk_df_storage(const jk_engine* e);
 
+/* Tiled storage only: caps on the block of fitted functions a mixed build
+ * contracts at once (its X block) and on the occupied slice of one FP64
+ * integral pass (0 = size them from free device memory, the default).  Small
+ * caps run the multi-block and multi-pass schedules on small systems. */
+int jk_df_set_tiled_blocks(jk_engine* e, int waux_max, int oc_max);
+
 /* Per-iteration part of compute_2body_fock_df (src/fockbuild.cpp:621-659):
  * J and K with respect to Cocc Cocc^T (the caller forms mult*(2J - K) as
  * Fock::formJKdf does at :173).  prec_mode 0 = FP64.  Host pointers. */
@@ -151,7 +157,11 @@ int jk_df_device(jk_engine* e, const double* dCocc, int nocc, int prec_mode, dou
 /* Per-stage device timing of DF builds (CUDA events on the launch stream;
  * molecular2 only has wall-clock timers, src/logger.cpp:35-40).
  * jk_stage_ms writes up to nmax stage durations of the last build (ms) and
- * their count to *nwritten.  FP64 stages are X = B C, K = X X^T, gamma, J. */
+ * their count to *nwritten.  Unpacked FP64 stages: X = B C, K = X X^T,
+ * gamma, J; unpacked mixed: GEMM1, GEMM2, J, finalize; tiled mixed: GEMM1
+ * total, GEMM2 total, J, finalize and (as a float) the number of
+ * fitted-function blocks; tiled FP64: first integral pass, its Y = L^-1 X',
+ * its K update, the remaining passes. */
 int jk_set_profiling(jk_engine* e, int on);
 int jk_stage_ms(jk_engine* e, float* ms, int nmax, int* nwritten);
 

@@ -334,7 +334,8 @@ void stage_mark(jk_engine* e, int k, cudaStream_t s) {
 
 int df_jk_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ, double* dK, cudaStream_t s) {
   DFState& d = e->df;
-  if (e->tiled.ready) return df_tiled_device(e, dC, nocc, mode, dJ, dK, s);
+  e->kev_blocks = 0;
+  if (e->tiled.metric_ready) return df_tiled_device(e, dC, nocc, mode, dJ, dK, s);
   if (!d.ready) return set_error(e, JK_ERR_STATE, "jk_df before jk_df_setup");
   if (mode == 1) return df_mixed_device(e, dC, nocc, dJ, dK, s);
   if (mode != 0) return set_error(e, JK_ERR_ARG, "jk_df: unsupported precision mode");
@@ -496,6 +497,27 @@ int jk_set_profiling(jk_engine* e, int on) {
 int jk_stage_ms(jk_engine* e, float* ms, int nmax, int* nwritten) {
   if (!e || !ms || !nwritten) return JK_ERR_ARG;
   *nwritten = 0;
+  if (e->profiling && e->kev_blocks > 0) {
+    // tiled mixed build: [GEMM1 total, GEMM2 total, J, finalize, fitted-function blocks]
+    const int B = e->kev_blocks;
+    cudaError_t st = cudaEventSynchronize(e->kev[3 * B + 1]);
+    if (st != cudaSuccess) return check_cuda(e, st, "kernel events");
+    float g1 = 0.f, g2 = 0.f, t = 0.f;
+    for (int b = 0; b < B; ++b) {
+      cudaEventElapsedTime(&t, e->kev[3 * b], e->kev[3 * b + 1]);
+      g1 += t;
+      cudaEventElapsedTime(&t, e->kev[3 * b + 1], e->kev[3 * b + 2]);
+      g2 += t;
+    }
+    float jt = 0.f, ft = 0.f;
+    cudaEventElapsedTime(&jt, e->kev[3 * B - 1], e->kev[3 * B]);
+    cudaEventElapsedTime(&ft, e->kev[3 * B], e->kev[3 * B + 1]);
+    const float vals[5] = {g1, g2, jt, ft, (float)B};
+    int k = 0;
+    for (; k < 5 && k < nmax; ++k) ms[k] = vals[k];
+    *nwritten = k;
+    return JK_OK;
+  }
   if (!e->profiling || e->nev_used < 2) return set_error(e, JK_ERR_STATE, "profiling off or no build recorded");
   cudaError_t st = cudaEventSynchronize(e->ev[e->nev_used - 1]);
   if (st != cudaSuccess) return check_cuda(e, st, "stage events");

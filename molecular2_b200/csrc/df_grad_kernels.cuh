@@ -69,7 +69,8 @@ struct Grad3Params {
   const double* sph_aux;
   const double* boys;
   int n;
-  const double* W3;       // [P][n][m] final basis: W3[(P * n + y) * n + x]
+  const double* W3;       // [P - w3_f0][n][m] final basis: W3[((P - w3_f0) * n + y) * n + x]
+  int w3_f0;              // first fitting function held in W3
   double* grad;           // 3 * natom
 };
 
@@ -91,7 +92,7 @@ __global__ void __launch_bounds__(64) k_grad3(const Grad3Params P) {
   for (int a = 0; a < dims[0]; ++a)
     for (int x = 0; x < dims[1]; ++x)
       for (int y = 0; y < dims[2]; ++y)
-        w0[(a * dims[1] + x) * dims[2] + y] = P.W3[((size_t)(f0 + a) * P.n + n0 + y) * P.n + m0 + x];
+        w0[(a * dims[1] + x) * dims[2] + y] = P.W3[((size_t)(f0 - P.w3_f0 + a) * P.n + n0 + y) * P.n + m0 + x];
   double* cur = w0;
   double* nxt = w1;
   for (int k = 0; k < 3; ++k)

@@ -586,6 +586,9 @@ static int tiled_mixed_prepare(jk_engine* e, int nocc) {
   cudaMemGetInfo(&fr, &tt);
   const double per_k = 4.0 * T.npad * NPX;  // hi + lo BF16
   int w = (int)std::min<double>(naux, std::max(64.0, 0.25 * fr / per_k));
+  if (T.waux_max > 0) w = std::min(w, T.waux_max);
+  // the X block must leave room for the zeroed tail of an odd last block
+  if (w < naux && (w & 1)) --w;
   w = std::max(1, std::min(naux, w));
   for (;; w = w / 2) {
     st = T.Xh.alloc((size_t)T.npad * w * NPX);
@@ -626,7 +629,20 @@ static int tiled_mixed(jk_engine* e, const double* dC, int nocc, double* dJ, dou
   cudaMemsetAsync(dJ, 0, sizeof(double) * n * n, s);
   st = cudaFuncSetAttribute(k_gemm1_sym, cudaFuncAttributeMaxDynamicSharedMemorySize, S1_SMEM);
   if (st != cudaSuccess) return check_cuda(e, st, "gemm1 attribute");
-  for (int k0 = 0; k0 < naux; k0 += T.waux) {
+  const int nblocks = (naux + T.waux - 1) / T.waux;
+  e->kev_blocks = 0;
+  auto kmark = [&](size_t k) {
+    if (!e->profiling) return;
+    while (e->kev.size() <= k) {
+      cudaEvent_t ev;
+      cudaEventCreate(&ev);
+      e->kev.push_back(ev);
+    }
+    cudaEventRecord(e->kev[k], s);
+  };
+  int blk = 0;
+  for (int k0 = 0; k0 < naux; k0 += T.waux, ++blk) {
+    kmark(3 * blk);
     const int w = std::min(T.waux, naux - k0);
     S1Params P{};
     P.nt = T.nt;
@@ -647,16 +663,31 @@ static int tiled_mixed(jk_engine* e, const double* dC, int nocc, double* dJ, dou
                                                                        T.maps[4], T.maps[5], P);
     st = cudaGetLastError();
     if (st != cudaSuccess) return check_cuda(e, st, "gemm1 (tiled) launch");
-    st = launch_gemm2(T.maps[6], T.maps[7], n, w * T.NPX / SBK, T.Kt.p, T.err.p, nsm, s);
+    kmark(3 * blk + 1);
+    // GEMM2 reads whole 64-wide k blocks: when w * NPX is not a multiple of
+    // 64 (odd w with an odd number of 160-orbital halves) the tail of each X
+    // row holds the previous block's values, so clear it
+    const int kbl = (w * T.NPX + SBK - 1) / SBK;
+    if (kbl * SBK != w * T.NPX) {
+      const size_t pitch = (size_t)T.waux * T.NPX * sizeof(__nv_bfloat16);
+      const size_t off = (size_t)w * T.NPX, width = (size_t)kbl * SBK - off;
+      cudaMemset2DAsync(T.Xh.p + off, pitch, 0, width * sizeof(__nv_bfloat16), T.npad, s);
+      cudaMemset2DAsync(T.Xl.p + off, pitch, 0, width * sizeof(__nv_bfloat16), T.npad, s);
+    }
+    st = launch_gemm2(T.maps[6], T.maps[7], n, kbl, T.Kt.p, T.err.p, nsm, s);
     if (st != cudaSuccess) return check_cuda(e, st, "gemm2 (tiled) launch");
+    kmark(3 * blk + 2);
   }
   stage_mark(e, 1, s);
   const int ksplit = 8, kchunk = (naux + ksplit - 1) / ksplit;
   k_J_tiles<<<dim3(T.npt, (unsigned)(TT / (JT_THREADS * 8)), ksplit), JT_THREADS, 0, s>>>(T.npt, naux, kchunk, n,
                                                                                         T.Bh.p, T.Bl.p, d.gamma.p, dJ);
   stage_mark(e, 2, s);
+  kmark(3 * nblocks);
   st = launch_finalize_mixed(n, T.Kt.p, dJ, dK, s);
   stage_mark(e, 3, s);
+  kmark(3 * nblocks + 1);
+  if (e->profiling) e->kev_blocks = nblocks;
   return check_cuda(e, st, "tiled mixed DF");
 }
 
@@ -754,6 +785,7 @@ static int tiled_fp64(jk_engine* e, const double* dC, int nocc, double* dJ, doub
   cudaMemGetInfo(&fr, &tt);
   const double per_o = 8.0 * (double)(npad + XB) * naux;
   int oc = (int)std::min<double>(nocc, std::floor(0.85 * (double)fr / per_o));
+  if (T.oc_max > 0) oc = std::min(oc, T.oc_max);
   if (oc < 1) return set_error(e, JK_ERR_NOMEM, "tiled FP64 DF: no room for one occupied orbital's X'");
   const int nch = (nocc + oc - 1) / oc;
   oc = (nocc + nch - 1) / nch;
@@ -800,6 +832,7 @@ static int tiled_fp64(jk_engine* e, const double* dC, int nocc, double* dJ, doub
       return JK_OK;
     });
     if (rc) return rc;
+    if (ch == 0) stage_mark(e, 1, s);  // profiling: first integral + X' pass
     if (ch == 0) {  // c = V^-1 d = L^-T (L^-1 d)
       DGemm g;
       g.M = naux;
@@ -847,6 +880,7 @@ static int tiled_fp64(jk_engine* e, const double* dC, int nocc, double* dJ, doub
                            cudaMemcpyDeviceToDevice, s);
       if (st != cudaSuccess) return check_cuda(e, st, "Y copy");
     }
+    if (ch == 0) stage_mark(e, 2, s);  // profiling: Y = L^-1 X' of the first slice
     // K += Y Y^T over (P, i)
     {
       const long long len = (long long)naux * ocur;
@@ -869,6 +903,7 @@ static int tiled_fp64(jk_engine* e, const double* dC, int nocc, double* dJ, doub
       k.ksplit = (int)std::max(1LL, std::min<long long>((2LL * nsm + tiles - 1) / tiles, len / 128));
       if ((st = dgemm(k, s)) != cudaSuccess) return check_cuda(e, st, "K += Y Y^T");
     }
+    if (ch == 0) stage_mark(e, 3, s);  // profiling: K of the first slice
   }
   if (nch == 1)  // J needs V^-1 d, known only after the first pass
     for (int t = 0; t < T.npt; ++t) {
@@ -879,16 +914,20 @@ static int tiled_fp64(jk_engine* e, const double* dC, int nocc, double* dJ, doub
     }
   mirror_lower(dJ, n, s);
   mirror_lower(dK, n, s);
-  stage_mark(e, 1, s);
+  stage_mark(e, 4, s);
   st = cudaGetLastError();
   if (st == cudaSuccess) st = cudaStreamSynchronize(s);  // scratch dies on return
   return check_cuda(e, st, "tiled FP64 DF");
 }
 
 int df_tiled_device(jk_engine* e, const double* dC, int nocc, int mode, double* dJ, double* dK, cudaStream_t s) {
-  if (!e->tiled.ready) return set_error(e, JK_ERR_STATE, "jk_df before jk_df_setup");
-  if (mode == 0) return tiled_fp64(e, dC, nocc, dJ, dK, s);
+  if (!e->tiled.metric_ready) return set_error(e, JK_ERR_STATE, "jk_df before jk_df_setup");
+  if (mode == 0) return tiled_fp64(e, dC, nocc, dJ, dK, s);  // needs only the metric
   if (mode != 1) return set_error(e, JK_ERR_ARG, "jk_df: unsupported precision mode");
+  if (!e->tiled.ready) {  // first mixed build after an FP64-only set-up: build the fitted tensor now
+    const int rc = df_tiled_setup(e);
+    if (rc) return rc;
+  }
   int rc = tiled_mixed(e, dC, nocc, dJ, dK, s);
   return rc ? rc : JK_OK;
 }
@@ -902,12 +941,22 @@ using namespace m2;
 extern "C" int jk_df_set_storage(jk_engine* e, int mode) {
   if (!e) return JK_ERR_ARG;
   if (mode < 0 || mode > 2) return set_error(e, JK_ERR_ARG, "jk_df_set_storage: mode must be 0, 1 or 2");
-  if (e->df.ready) return set_error(e, JK_ERR_STATE, "jk_df_set_storage after jk_df_setup");
+  if (e->df.ready || e->tiled.metric_ready)
+    return set_error(e, JK_ERR_STATE, "jk_df_set_storage after jk_df_setup");
   e->df_storage = mode;
+  return JK_OK;
+}
+
+extern "C" int jk_df_set_tiled_blocks(jk_engine* e, int waux_max, int oc_max) {
+  if (!e) return JK_ERR_ARG;
+  if (waux_max < 0 || oc_max < 0) return set_error(e, JK_ERR_ARG, "jk_df_set_tiled_blocks: negative cap");
+  e->tiled.waux_max = waux_max;
+  e->tiled.oc_max = oc_max;
+  e->tiled.NPX = 0;  // re-plan the mixed scratch on the next build
   return JK_OK;
 }
 
 extern "C" int jk_df_storage(const jk_engine* e) {
   if (!e) return -1;
-  return e->tiled.ready ? 2 : (e->df.ready ? 1 : 0);
+  return (e->tiled.ready || e->tiled.metric_ready) ? 2 : (e->df.ready ? 1 : 0);
 }

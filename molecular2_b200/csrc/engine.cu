@@ -371,6 +371,7 @@ void jk_destroy(jk_engine* e) {
   if (e->cusolver) cusolverDnDestroy(e->cusolver);
   for (auto& ev : e->ev)
     if (ev) cudaEventDestroy(ev);
+  for (auto& ev : e->kev) cudaEventDestroy(ev);
   cudaStream_t s = e->stream;
   delete e;  // frees device buffers
   if (s) cudaStreamDestroy(s);

@@ -116,6 +116,7 @@ struct TiledDF {
   DevBuf<__nv_bfloat16> Bh, Bl;      // [K][t][r][c]
   // mixed-build scratch
   int NPX = 0, waux = 0, nocc = 0;   // X row length per K (nhalf * 160), aux block, occupied count
+  int waux_max = 0, oc_max = 0;      // caps on the aux block and the FP64 occupied slice (0: memory decides)
   DevBuf<__nv_bfloat16> Ch, Cl;      // [i][y], NPX x npad
   DevBuf<__nv_bfloat16> Xh, Xl;      // [x][K_local][i], npad x waux x NPX
   DevBuf<double> Kt;                 // n x n lower-tile K
@@ -166,6 +167,10 @@ struct jk_engine {
   static constexpr int NSTAGE_EV = 8;
   cudaEvent_t ev[NSTAGE_EV] = {};
   int nev_used = 0;
+  // tiled mixed builds time each kernel launch (per fitted-function block:
+  // GEMM1 start, GEMM2 start, GEMM2 end; then J end and finalize end)
+  std::vector<cudaEvent_t> kev;
+  int kev_blocks = 0;
 };
 
 namespace m2 {

@@ -132,6 +132,10 @@ struct Ring {
   }
   size_t size() const { return order.size(); }
   double* operator[](size_t i) const { return order[i]; }
+  void clear() {
+    for (double* p : order) spare.push_back(p);
+    order.clear();
+  }
 };
 
 struct Diis {  // DIISEngine (src/diis.cpp) with error vectors in HBM
@@ -158,6 +162,12 @@ struct Diis {  // DIISEngine (src/diis.cpp) with error vectors in HBM
     full_piv_solve(nB, size, w, x, rank);
     x.push_back((double)rank);
     return x;
+  }
+
+  void reset() {
+    errs.clear();
+    lastB.assign(1, 0.0);
+    lastB_dim = 1;
   }
 
   std::vector<double> compute(Gpu& g, const double* err, size_t len) {
@@ -210,8 +220,10 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   if (nocc <= 0 || nocc > n) return set_error(e, JK_ERR_ARG, "scf: nocc out of range");
   if (o->df && (e->df.k0 != 0 || (e->df.k1 >= 0 && e->df.k1 != e->aux.n_final)))
     return set_error(e, JK_ERR_STATE, "scf: the DF SCF needs the whole fitting range (jk_df_set_range)");
-  if (o->df && !e->df.ready) {
-    int rc = df_setup(e);
+  if (o->df && !e->df.ready && !e->tiled.metric_ready) {
+    // tiled storage with FP64 builds only needs the metric; mixed builds
+    // build the fitted tensor on their first call
+    int rc = (o->prec_mode == 0 && df_use_tiled(e)) ? df_tiled_metric(e) : df_setup(e);
     if (rc) return rc;
   }
   cudaStream_t s = e->stream;
@@ -283,8 +295,11 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   // set by the mixed builds' own error), FP64 builds after that.  With
   // mixed_refresh > 0 the later iterations instead use Gmixed(D) + Delta, where
   // Delta = G64 - Gmixed is taken from one FP64 and one mixed build at the same
-  // density every mixed_refresh iterations, and the reported energy comes from a
-  // final FP64 build at the converged density.
+  // density at the switch and then every mixed_refresh iterations (the DIIS
+  // history restarts with each new Delta), and the reported energy comes from
+  // a final FP64 build at the converged density: the energy is stationary in
+  // D, so the density error the corrected builds leave enters it squared.
+  // Convergence needs two corrected iterations after the last refresh.
   const bool mixed = o->df && o->prec_mode == 1;
   const double mixed_switch = o->mixed_switch > 0.0 ? o->mixed_switch : 1e-3;
   const int refresh_every = o->mixed_refresh > 0 ? o->mixed_refresh : 0;
@@ -460,6 +475,10 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
         have_delta = true;
         since_refresh = 0;
         ++refreshes;
+        // the Fock matrices in the DIIS history lack this correction
+        focks.clear();
+        diis.reset();
+        fock_iter = 0;
       } else if (corrected) {
         if ((rc2 = jk(nullptr, t2.p, 1))) return rc2;
         g.axpy(1.0, Delta.p, t2.p, nn);
@@ -545,7 +564,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     if (it > 2) average(weights);
     transform(F.p);
     // a mixed run converges only on FP64 (or FP64-corrected) builds
-    const bool precise = !mixed || (corrected ? (have_delta && refreshes >= 2) : fp64_after_switch >= 2);
+    const bool precise = !mixed || (corrected ? (have_delta && since_refresh >= 2) : fp64_after_switch >= 2);
     converged = dd < o->densconverge && delta < o->enconverge && precise;
     ++it;
   }

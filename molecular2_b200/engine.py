@@ -44,6 +44,7 @@ SIGNATURES = {
     "jk_df_set_range": (_I, [_P, _I, _I]),
     "jk_df_set_storage": (_I, [_P, _I]),
     "jk_df_storage": (_I, [_P]),
+    "jk_df_set_tiled_blocks": (_I, [_P, _I, _I]),
     "jk_df": (_I, [_P, _P, _I, _I, _P, _P]),
     "jk_df_device": (_I, [_P, _P, _I, _I, _P, _P, _P]),
     "jk_one_body": (_I, [_P, _P, _P, _P]),
@@ -201,6 +202,11 @@ class IntegralEngine:
         FP64 build streaming the integrals, or "auto" (tiled when the unpacked
         tensor would not fit on the device)."""
         self._check(self.lib.jk_df_set_storage(self.h, self.DF_STORAGE[mode]))
+
+    def set_tiled_blocks(self, waux_max=0, oc_max=0):
+        """Caps on the mixed build's fitted-function block and the FP64 build's
+        occupied slice for tiled storage (0: sized from free device memory)."""
+        self._check(self.lib.jk_df_set_tiled_blocks(self.h, waux_max, oc_max))
 
     @property
     def df_storage(self):
