@@ -587,12 +587,13 @@ static int tiled_mixed_prepare(jk_engine* e, int nocc) {
   const double per_k = 4.0 * T.npad * NPX;  // hi + lo BF16
   int w = (int)std::min<double>(naux, std::max(64.0, 0.25 * fr / per_k));
   if (T.waux_max > 0) w = std::min(w, T.waux_max);
-  // the X block must leave room for the zeroed tail of an odd last block
-  if (w < naux && (w & 1)) --w;
   w = std::max(1, std::min(naux, w));
+  // X rows are padded to an even number of fitted functions, so that a row
+  // is a whole number of 64-wide k blocks (NPX is a multiple of 160)
   for (;; w = w / 2) {
-    st = T.Xh.alloc((size_t)T.npad * w * NPX);
-    if (st == cudaSuccess) st = T.Xl.alloc((size_t)T.npad * w * NPX);
+    const int ws = w + (w & 1);
+    st = T.Xh.alloc((size_t)T.npad * ws * NPX);
+    if (st == cudaSuccess) st = T.Xl.alloc((size_t)T.npad * ws * NPX);
     if (st == cudaSuccess) break;
     T.Xh.reset();
     T.Xl.reset();
@@ -600,13 +601,14 @@ static int tiled_mixed_prepare(jk_engine* e, int nocc) {
     if (w <= 16) return check_cuda(e, st, "tiled mixed X block");
   }
   T.waux = w;
+  T.wstride = w + (w & 1);
   cudaMemsetAsync(T.err.p, 0, sizeof(int), e->stream);
   const uint64_t brows = (uint64_t)naux * T.npt * TB;
   bool ok = make_map(&T.maps[0], T.Bh.p, TB, brows, SBK, TB) && make_map(&T.maps[1], T.Bl.p, TB, brows, SBK, TB) &&
             make_map(&T.maps[2], T.Bh.p, TB, brows, SBK, SBK) && make_map(&T.maps[3], T.Bl.p, TB, brows, SBK, SBK) &&
             make_map(&T.maps[4], T.Ch.p, T.npad, NPX, SBK, SN) && make_map(&T.maps[5], T.Cl.p, T.npad, NPX, SBK, SN) &&
-            make_map(&T.maps[6], T.Xh.p, (uint64_t)w * NPX, T.npad, SBK, TB) &&
-            make_map(&T.maps[7], T.Xl.p, (uint64_t)w * NPX, T.npad, SBK, TB);
+            make_map(&T.maps[6], T.Xh.p, (uint64_t)T.wstride * NPX, T.npad, SBK, TB) &&
+            make_map(&T.maps[7], T.Xl.p, (uint64_t)T.wstride * NPX, T.npad, SBK, TB);
   if (!ok) return set_error(e, JK_ERR_CUDA, "cuTensorMapEncodeTiled failed (tiled DF)");
   T.NPX = NPX;
   T.nocc = nocc;
@@ -648,7 +650,7 @@ static int tiled_mixed(jk_engine* e, const double* dC, int nocc, double* dJ, dou
     P.nt = T.nt;
     P.npt = T.npt;
     P.k0 = k0;
-    P.wstride = T.waux;
+    P.wstride = T.wstride;
     P.nhalf = T.NPX / SN;
     P.nitems = w * T.nt * P.nhalf;
     P.nocc = nocc;
@@ -669,7 +671,7 @@ static int tiled_mixed(jk_engine* e, const double* dC, int nocc, double* dJ, dou
     // row holds the previous block's values, so clear it
     const int kbl = (w * T.NPX + SBK - 1) / SBK;
     if (kbl * SBK != w * T.NPX) {
-      const size_t pitch = (size_t)T.waux * T.NPX * sizeof(__nv_bfloat16);
+      const size_t pitch = (size_t)T.wstride * T.NPX * sizeof(__nv_bfloat16);
       const size_t off = (size_t)w * T.NPX, width = (size_t)kbl * SBK - off;
       cudaMemset2DAsync(T.Xh.p + off, pitch, 0, width * sizeof(__nv_bfloat16), T.npad, s);
       cudaMemset2DAsync(T.Xl.p + off, pitch, 0, width * sizeof(__nv_bfloat16), T.npad, s);

@@ -116,6 +116,7 @@ struct TiledDF {
   DevBuf<__nv_bfloat16> Bh, Bl;      // [K][t][r][c]
   // mixed-build scratch
   int NPX = 0, waux = 0, nocc = 0;   // X row length per K (nhalf * 160), aux block, occupied count
+  int wstride = 0;                   // X row stride in fitted functions (waux rounded up to even)
   int waux_max = 0, oc_max = 0;      // caps on the aux block and the FP64 occupied slice (0: memory decides)
   DevBuf<__nv_bfloat16> Ch, Cl;      // [i][y], NPX x npad
   DevBuf<__nv_bfloat16> Xh, Xl;      // [x][K_local][i], npad x waux x NPX
