@@ -82,6 +82,18 @@ int jk_direct(jk_engine* e, const double* D, double precision, double multiplier
 int jk_direct_device(jk_engine* e, const double* dD, double precision, double multiplier, double* dJ,
                      double* dK, void* stream);
 
+/* Unrestricted (UHF) integral-direct J and K: J[Da], J[Db], K[Da], K[Db] from
+ * one pass over the shell quartets, screened with the shell-block norms of
+ * Da + Db, every integral batch digested into both densities.  Each result is
+ * w.r.t. its full spin density and scaled by `multiplier`; the caller forms
+ * J - K per spin as molecular2 does.  Replaces
+ * UnrestrictedFock::formJKdirect(Schwarz, Da, Db, multiplier)
+ * (src/fockbuild.cpp:266-362). */
+int jk_direct_uhf(jk_engine* e, const double* Da, const double* Db, double precision, double multiplier, double* Ja,
+                  double* Jb, double* Ka, double* Kb);
+int jk_direct_uhf_device(jk_engine* e, const double* dDa, const double* dDb, double precision, double multiplier,
+                         double* dJa, double* dJb, double* dKa, double* dKb, void* stream);
+
 /* Integral-direct J and K exactly as jk_direct_device, for callers that must
  * not allocate device memory while building a Fock matrix: for example a
  * service that reserves all device memory for a caching allocator at start-up
@@ -104,6 +116,14 @@ int jk_direct_noalloc(jk_engine* e, const double* dD, double precision, double m
 /* Number of shell quartets the last direct build (jk_direct, jk_direct_device
  * or jk_direct_noalloc) evaluated; -1 before the first build. */
 long long jk_last_quartets(const jk_engine* e);
+
+/* Work counts of the last jk_direct / jk_direct_device / jk_direct_uhf build
+ * per (bra, ket) shell-pair class, classes ordered ss, ps, pp, ds, dp, dd:
+ * out[3 (bra * 6 + ket) + k] for k = 0 quartets, 1 bra primitive pairs summed
+ * over them, 2 primitive quartets; up to nmax values, count in *nwritten.
+ * JK_ERR_STATE after jk_direct_noalloc (it keeps no counters).  molecular2
+ * has no counterpart; these give the flop model of the roofline. */
+int jk_last_class_work(const jk_engine* e, long long* out, int nmax, int* nwritten);
 
 /* Three-index integrals (P|mn) in molecular2's packed layout: column-major
  * (n(n+1)/2) x naux, row x(x+1)/2 + y for x >= y.
@@ -128,6 +148,16 @@ int jk_df_setup(jk_engine* e);
  * range (JK_ERR_STATE otherwise).  Replaces nothing in molecular2, whose DF
  * build is serial (src/fockbuild.cpp:621-659). */
 int jk_df_set_range(jk_engine* e, int k0, int k1);
+
+/* Unrestricted (UHF) DF J and K: the jk_df build for the alpha occupied
+ * orbitals Ca (n x na) and for the beta ones Cb (n x nb) over the same fitted
+ * tensor, all four scaled by `multiplier` (nb = 0 gives zero beta matrices).
+ * Replaces UnrestrictedFock::formJKdf(ca_occ, cb_occ, multiplier)
+ * (src/fockbuild.cpp:365-372). */
+int jk_df_uhf(jk_engine* e, const double* Ca, int na, const double* Cb, int nb, int prec_mode, double multiplier,
+              double* Ja, double* Jb, double* Ka, double* Kb);
+int jk_df_uhf_device(jk_engine* e, const double* dCa, int na, const double* dCb, int nb, int prec_mode,
+                     double multiplier, double* dJa, double* dJb, double* dKa, double* dKb, void* stream);
 
 /* Layout of the fitted tensor, chosen before jk_df_setup (molecular2 keeps one
  * packed FP64 (n(n+1)/2) x naux matrix, src/fockbuild.cpp:598-619, which
@@ -208,6 +238,12 @@ typedef struct jk_scf_options {
   double* out_density;     /* optional host n x n */
   double* out_coeffs;      /* optional host n x n (MO coefficients, columns) */
   double* out_eps;         /* optional host n */
+  double* out_trace;       /* optional host maxiter x 5, per iteration: energy, ||D - D_old||_F, rms of the
+                              DIIS error, build kind (0 FP64, 1 mixed, 2 mixed + correction, 3 correction
+                              refresh: mixed and FP64 builds), ||D||_F */
+  double lindep;           /* 0 (default): symmetric S^-1/2 over all directions as molecular2
+                              (src/fock.cpp:124-142); > 0: canonical orthogonalisation dropping the
+                              directions whose overlap eigenvalue is <= lindep */
 } jk_scf_options;
 
 typedef struct jk_scf_result {
@@ -221,6 +257,7 @@ typedef struct jk_scf_result {
   double last_delta_d;
   int mixed_builds;        /* J/K builds done in mixed precision */
   double diag_ms;          /* device time in the Fock diagonalisations */
+  int lindep_dropped;      /* directions removed by jk_scf_options.lindep */
 } jk_scf_result;
 
 int jk_scf_rhf(jk_engine* e, const jk_scf_options* opt, jk_scf_result* res);

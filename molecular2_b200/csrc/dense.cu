@@ -6,8 +6,9 @@
 // ring by cp.async (8-byte copies, so any stride works; the thread-to-element
 // map follows whichever operand dimension is contiguous so the copies
 // coalesce).  Out-of-range elements are copied as zeros (cp.async with
-// source size 0).  Shared rows are 136 doubles long, so the 32 lanes of a
-// fragment load (4 k rows x 8 consecutive m) fall in two bank wavefronts.
+// source size 0).  The shared-memory pitches (136 doubles for [k][m], 20 for
+// [m][k] tiles) put the 32 lanes of a fragment load (4 k x 8 consecutive m)
+// and of a copy into the fewest bank wavefronts.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -19,8 +20,10 @@ namespace m2 {
 namespace {
 
 constexpr int GBM = 128, GBN = 128, GBK = 16, GT = 256;
-constexpr int LDS = GBM + 8;  // padded shared row (doubles): 1088 B, 16-byte aligned, conflict-free fragments
-constexpr int GSMEM = 4 * GBK * LDS * (int)sizeof(double);  // A and B, two buffers each
+constexpr int LDS = GBM + 8;   // [k][m] rows (doubles): 1088 B, 16-byte aligned, conflict-free fragments
+constexpr int LDK = GBK + 4;   // [m][k] rows (doubles): 160 B, so 4 rows of 4 k fill the 32 banks once
+constexpr int OPER = (GBK * LDS > GBM * LDK) ? GBK * LDS : GBM * LDK;  // doubles per operand buffer
+constexpr int GSMEM = 4 * OPER * (int)sizeof(double);                  // A and B, two buffers each
 
 __device__ __forceinline__ void cp8(double* dst, const double* src, bool ok) {
   const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
@@ -44,11 +47,17 @@ __device__ __forceinline__ void tri_tile(int t, int& tm, int& tn) {
   tn = t - m * (m + 1) / 2;
 }
 
+// Operand tiles in shared memory follow the operand's contiguous dimension in
+// global memory: an operand whose k is contiguous (AK1 for A, !BN1 for B) is
+// kept as [m][k] (pitch LDK), the other as [k][m] (pitch LDS), so that the
+// 8-byte copies of a warp land in distinct banks.
 template <bool AK1, bool BN1>
 __global__ void __launch_bounds__(GT) k_dgemm(const DGemm g, int tiles_n) {
   extern __shared__ __align__(16) double gsm[];
-  double(*As)[GBK][LDS] = reinterpret_cast<double(*)[GBK][LDS]>(gsm);
-  double(*Bs)[GBK][LDS] = reinterpret_cast<double(*)[GBK][LDS]>(gsm + 2 * GBK * LDS);
+  double* As = gsm;             // two buffers of OPER doubles
+  double* Bs = gsm + 2 * OPER;
+  auto aidx = [](int buf, int k, int m) { return buf * OPER + (AK1 ? m * LDK + k : k * LDS + m); };
+  auto bidx = [](int buf, int k, int n) { return buf * OPER + (BN1 ? k * LDS + n : n * LDK + k); };
   int tm, tn;
   if (g.c_lower)
     tri_tile(blockIdx.x, tm, tn);
@@ -89,7 +98,7 @@ __global__ void __launch_bounds__(GT) k_dgemm(const DGemm g, int tiles_n) {
       }
       const int gm = m0 + m, gk = k0 + k;
       const bool ok = gm < g.M && gk < ke;
-      cp8(&As[buf][k][m], ok ? A + (long long)gm * g.sam + (long long)gk * g.sak : A, ok);
+      cp8(As + aidx(buf, k, m), ok ? A + (long long)gm * g.sam + (long long)gk * g.sak : A, ok);
     }
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
@@ -103,7 +112,7 @@ __global__ void __launch_bounds__(GT) k_dgemm(const DGemm g, int tiles_n) {
       }
       const int gn = n0 + n, gk = k0 + k;
       const bool ok = gn < g.N && gk < ke;
-      cp8(&Bs[buf][k][n], ok ? B + (long long)gk * g.sbk + (long long)gn * g.sbn : B, ok);
+      cp8(Bs + bidx(buf, k, n), ok ? B + (long long)gk * g.sbk + (long long)gn * g.sbn : B, ok);
     }
   };
 
@@ -127,9 +136,9 @@ __global__ void __launch_bounds__(GT) k_dgemm(const DGemm g, int tiles_n) {
     for (int k4 = 0; k4 < GBK; k4 += 4) {
       double a[8], b[4];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) a[i] = As[buf][k4 + fk][wm * 64 + i * 8 + fr];
+      for (int i = 0; i < 8; ++i) a[i] = As[aidx(buf, k4 + fk, wm * 64 + i * 8 + fr)];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[buf][k4 + fk][wn * 32 + j * 8 + fr];
+      for (int j = 0; j < 4; ++j) b[j] = Bs[bidx(buf, k4 + fk, wn * 32 + j * 8 + fr)];
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll

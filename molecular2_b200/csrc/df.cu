@@ -226,6 +226,11 @@ __global__ void __launch_bounds__(DFJ_THREADS) k_df_J_lower(int n, int naux, int
   }
 }
 
+__global__ void k_scale_mat(size_t n, double a, double* x) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] *= a;
+}
+
 // upper triangle of a column-major symmetric matrix from its lower triangle
 __global__ void k_mirror_lower(int n, double* J) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -485,6 +490,60 @@ int jk_df(jk_engine* e, const double* C, int nocc, int prec_mode, double* J, dou
   if (st == cudaSuccess) st = cudaMemcpyAsync(K, e->Kfinal.p, sizeof(double) * n * n, cudaMemcpyDeviceToHost, e->stream);
   if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
   if (st != cudaSuccess) return check_cuda(e, st, "jk_df download");
+  return prec_mode == 1 ? df_mixed_error(e) : JK_OK;
+}
+
+int jk_df_uhf_device(jk_engine* e, const double* dCa, int na, const double* dCb, int nb, int prec_mode,
+                     double multiplier, double* dJa, double* dJb, double* dKa, double* dKb, void* stream) {
+  if (!e || !dJa || !dJb || !dKa || !dKb || na < 0 || nb < 0 || (na > 0 && !dCa) || (nb > 0 && !dCb))
+    return JK_ERR_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+  const int n = e->obs.n_final;
+  const size_t nn = (size_t)n * n;
+  // UnrestrictedFock::formJKdf (src/fockbuild.cpp:365-372): compute_2body_fock_df
+  // for each spin over the same fitted tensor, then both scaled by multiplier
+  const double* Cs[2] = {dCa, dCb};
+  const int no[2] = {na, nb};
+  double* Js[2] = {dJa, dJb};
+  double* Ks[2] = {dKa, dKb};
+  for (int k = 0; k < 2; ++k) {
+    if (no[k] == 0) {
+      cudaMemsetAsync(Js[k], 0, sizeof(double) * nn, s);
+      cudaMemsetAsync(Ks[k], 0, sizeof(double) * nn, s);
+      continue;
+    }
+    int rc = df_jk_device(e, Cs[k], no[k], prec_mode, Js[k], Ks[k], s);
+    if (rc) return rc;
+    if (multiplier != 1.0) {
+      k_scale_mat<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(nn, multiplier, Js[k]);
+      k_scale_mat<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(nn, multiplier, Ks[k]);
+    }
+  }
+  return check_cuda(e, cudaGetLastError(), "jk_df_uhf");
+}
+
+int jk_df_uhf(jk_engine* e, const double* Ca, int na, const double* Cb, int nb, int prec_mode, double multiplier,
+              double* Ja, double* Jb, double* Ka, double* Kb) {
+  if (!e || !Ja || !Jb || !Ka || !Kb || na < 0 || nb < 0 || (na > 0 && !Ca) || (nb > 0 && !Cb)) return JK_ERR_ARG;
+  const int n = e->obs.n_final;
+  const size_t nn = (size_t)n * n;
+  DevBuf<double> d;
+  cudaError_t st = d.alloc(4 * nn + (size_t)n * (na + nb));
+  double* dCa = d.p + 4 * nn;
+  double* dCb = dCa + (size_t)n * na;
+  if (st == cudaSuccess && na)
+    st = cudaMemcpyAsync(dCa, Ca, sizeof(double) * n * na, cudaMemcpyHostToDevice, e->stream);
+  if (st == cudaSuccess && nb)
+    st = cudaMemcpyAsync(dCb, Cb, sizeof(double) * n * nb, cudaMemcpyHostToDevice, e->stream);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_df_uhf upload");
+  int rc = jk_df_uhf_device(e, dCa, na, dCb, nb, prec_mode, multiplier, d.p, d.p + nn, d.p + 2 * nn, d.p + 3 * nn,
+                            nullptr);
+  if (rc) return rc;
+  double* outs[4] = {Ja, Jb, Ka, Kb};
+  for (int k = 0; k < 4 && st == cudaSuccess; ++k)
+    st = cudaMemcpyAsync(outs[k], d.p + k * nn, sizeof(double) * nn, cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_df_uhf download");
   return prec_mode == 1 ? df_mixed_error(e) : JK_OK;
 }
 

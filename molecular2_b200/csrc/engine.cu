@@ -298,6 +298,15 @@ void launch_cart_to_final_sym(const jk_engine* e, const double* Xcart, double sc
                                            Xfinal);
 }
 
+__global__ void k_add(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ c, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) c[i] = a[i] + b[i];
+}
+
+void launch_add(const double* a, const double* b, double* c, size_t n, cudaStream_t s) {
+  k_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, b, c, n);
+}
+
 void launch_shell_norms(const jk_engine* e, const double* Dfinal, double* Dnorm, double* Dmax, cudaStream_t s) {
   const int ns = e->obs.nshell, n = e->obs.n_final;
   cudaMemsetAsync(Dmax, 0, sizeof(double), s);

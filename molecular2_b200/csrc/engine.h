@@ -163,6 +163,10 @@ struct jk_engine {
   // quartet counter of the last direct build (engine scratch or the fixed
   // array of jk_direct_noalloc), read by jk_last_quartets
   const unsigned long long* last_counter = nullptr;
+  // per (bra, ket) pair class of the last direct build: quartets, bra
+  // primitive pairs and primitive quartets evaluated (the work model's counts)
+  m2::DevBuf<unsigned long long> class_work;
+  bool class_work_valid = false;
   // optional per-stage CUDA-event timing of the DF build (jk_set_profiling)
   bool profiling = false;
   static constexpr int NSTAGE_EV = 8;
@@ -214,4 +218,7 @@ int df_tiled_error(jk_engine* e);
 void launch_final_to_cart(const jk_engine* e, const double* Dfinal, double* Dcart, cudaStream_t s);
 void launch_cart_to_final_sym(const jk_engine* e, const double* Xcart, double scale, double* Xfinal, cudaStream_t s);
 void launch_shell_norms(const jk_engine* e, const double* Dfinal, double* Dnorm, double* Dmax, cudaStream_t s);
+void launch_add(const double* a, const double* b, double* c, size_t n, cudaStream_t s);  // c = a + b
+int direct_jk_uhf_device(jk_engine* e, const double* dDa, const double* dDb, double precision, double mult,
+                         double* dJa, double* dJb, double* dKa, double* dKb, cudaStream_t s);
 }  // namespace m2

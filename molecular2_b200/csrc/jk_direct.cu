@@ -164,20 +164,20 @@ static int ket_chunk(int nbra, int nket_max) {
   return k;
 }
 
-static void launch_jk(int A, int B, const JKParams& Pin, int nbra, int nket_max, cudaStream_t s) {
+static void launch_jk(int A, int B, const JKParams& Pin, int nbra, int nket_max, cudaStream_t s, int nden = 1) {
   JKParams P = Pin;
   P.kchunk = ket_chunk(nbra, nket_max);
   dim3 grid(nbra, (nket_max + P.kchunk - 1) / P.kchunk);
   if (A <= 2)
-    launch_jk_bra_s(A, B, P, grid, s);
+    launch_jk_bra_s(A, B, nden, P, grid, s);
   else if (A == 3)
-    launch_jk_bra_ds(B, P, grid, s);
+    launch_jk_bra_ds(B, nden, P, grid, s);
   else if (A == 4)
-    launch_jk_bra_dp(B, P, grid, s);
+    launch_jk_bra_dp(B, nden, P, grid, s);
   else if (B < 4)
-    launch_jk_bra_dd_lo(B, P, grid, s);
+    launch_jk_bra_dd_lo(B, nden, P, grid, s);
   else
-    launch_jk_bra_dd_hi(B, P, grid, s);
+    launch_jk_bra_dd_hi(B, nden, P, grid, s);
 }
 
 int direct_jk_device(jk_engine* e, const double* dD, double precision, double mult, double* dJ, double* dK,
@@ -197,6 +197,10 @@ int direct_jk_device(jk_engine* e, const double* dD, double precision, double mu
   unsigned long long* counter = reinterpret_cast<unsigned long long*>(e->Dmax.p + 1);
   e->last_counter = counter;
   cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+  if ((st = e->class_work.alloc(3 * NPAIRCLASS * NPAIRCLASS)) != cudaSuccess)
+    return check_cuda(e, st, "jk_direct work counters");
+  cudaMemsetAsync(e->class_work.p, 0, sizeof(unsigned long long) * 3 * NPAIRCLASS * NPAIRCLASS, s);
+  e->class_work_valid = true;
   JKParams P{};
   P.pp = prim_view(e);
   P.sh = shell_view(e);
@@ -207,6 +211,7 @@ int direct_jk_device(jk_engine* e, const double* dD, double precision, double mu
   P.nc = nc;
   P.Jc = e->Jcart.p;
   P.Kc = e->Kcart.p;
+  P.dstride = (size_t)nc * nc;
   P.precision = precision;
   P.boys = e->boys.p;
   P.counter = counter;
@@ -219,12 +224,76 @@ int direct_jk_device(jk_engine* e, const double* dD, double precision, double mu
       P.bra = view(bra);
       P.ket = view(ket);
       P.same_class = (A == B);
+      P.work = e->class_work.p + 3 * (A * NPAIRCLASS + B);
       launch_jk(A, B, P, bra.npair, ket.npair, s);
     }
   // J = 1/4 (J + J^T) mult, K = 1/2 * 1/4 (K + K^T) mult  (src/fockbuild.cpp:146-149, 161-162)
   launch_cart_to_final_sym(e, e->Jcart.p, 0.25 * mult, dJ, s);
   launch_cart_to_final_sym(e, e->Kcart.p, 0.125 * mult, dK, s);
   return check_cuda(e, cudaGetLastError(), "jk_direct launch");
+}
+
+// J and K of two densities (UHF alpha and beta) from one pass over the shell
+// quartets: UnrestrictedFock::formJKdirect (src/fockbuild.cpp:266-362), which
+// screens with the shell-block norms of Da + Db and digests both densities from
+// each integral batch.  Each J, K is w.r.t. its own full density.
+int direct_jk_uhf_device(jk_engine* e, const double* dDa, const double* dDb, double precision, double mult,
+                         double* dJa, double* dJb, double* dKa, double* dKb, cudaStream_t s) {
+  const int n = e->obs.n_final, nc = e->obs.n_cart, ns = e->obs.nshell;
+  const size_t ncc = (size_t)nc * nc, nn = (size_t)n * n;
+  DevBuf<double> Dsum, Dc2, Jc2, Kc2;
+  cudaError_t st = Dsum.alloc(nn);
+  if (st == cudaSuccess) st = Dc2.alloc(2 * ncc);
+  if (st == cudaSuccess) st = Jc2.alloc(2 * ncc);
+  if (st == cudaSuccess) st = Kc2.alloc(2 * ncc);
+  if (st == cudaSuccess) st = e->Dnorm.alloc((size_t)ns * ns);
+  if (st == cudaSuccess) st = e->Dmax.alloc(2);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_direct_uhf scratch");
+  launch_add(dDa, dDb, Dsum.p, nn, s);
+  launch_shell_norms(e, Dsum.p, e->Dnorm.p, e->Dmax.p, s);
+  launch_final_to_cart(e, dDa, Dc2.p, s);
+  launch_final_to_cart(e, dDb, Dc2.p + ncc, s);
+  cudaMemsetAsync(Jc2.p, 0, sizeof(double) * 2 * ncc, s);
+  cudaMemsetAsync(Kc2.p, 0, sizeof(double) * 2 * ncc, s);
+  unsigned long long* counter = reinterpret_cast<unsigned long long*>(e->Dmax.p + 1);
+  e->last_counter = counter;
+  cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+  JKParams P{};
+  P.pp = prim_view(e);
+  P.sh = shell_view(e);
+  P.Dnorm = e->Dnorm.p;
+  P.nshell = ns;
+  P.Dmax = e->Dmax.p;
+  P.Dc = Dc2.p;
+  P.nc = nc;
+  P.Jc = Jc2.p;
+  P.Kc = Kc2.p;
+  P.dstride = ncc;
+  P.precision = precision;
+  P.boys = e->boys.p;
+  P.counter = counter;
+  if ((st = e->class_work.alloc(3 * NPAIRCLASS * NPAIRCLASS)) != cudaSuccess)
+    return check_cuda(e, st, "jk_direct_uhf work counters");
+  cudaMemsetAsync(e->class_work.p, 0, sizeof(unsigned long long) * 3 * NPAIRCLASS * NPAIRCLASS, s);
+  e->class_work_valid = true;
+  for (int A = 0; A < NPAIRCLASS; ++A)
+    for (int B = 0; B <= A; ++B) {
+      const PairClassDev& bra = e->pcls[A];
+      const PairClassDev& ket = e->pcls[B];
+      if (bra.npair == 0 || ket.npair == 0) continue;
+      P.bra = view(bra);
+      P.ket = view(ket);
+      P.same_class = (A == B);
+      P.work = e->class_work.p + 3 * (A * NPAIRCLASS + B);
+      launch_jk(A, B, P, bra.npair, ket.npair, s, 2);
+    }
+  launch_cart_to_final_sym(e, Jc2.p, 0.25 * mult, dJa, s);
+  launch_cart_to_final_sym(e, Jc2.p + ncc, 0.25 * mult, dJb, s);
+  launch_cart_to_final_sym(e, Kc2.p, 0.125 * mult, dKa, s);
+  launch_cart_to_final_sym(e, Kc2.p + ncc, 0.125 * mult, dKb, s);
+  st = cudaGetLastError();
+  if (st == cudaSuccess) st = cudaStreamSynchronize(s);  // the scratch dies on return
+  return check_cuda(e, st, "jk_direct_uhf");
 }
 
 // ---------------------------------------------------------------- no-allocation variant
@@ -288,6 +357,7 @@ int direct_jk_noalloc(jk_engine* e, const double* dD, double precision, double m
   double* Dmax = Dn + NOALLOC_SS;
   unsigned long long* counter = reinterpret_cast<unsigned long long*>(Dmax + 1);
   e->last_counter = counter;
+  e->class_work_valid = false;  // this build keeps no per-class counters
   // the array keeps the previous call's contents: clear the accumulators
   launch_shell_norms(e, dD, Dn, Dmax, s);  // zeroes Dmax itself
   launch_final_to_cart(e, dD, Dc, s);
@@ -307,6 +377,7 @@ int direct_jk_noalloc(jk_engine* e, const double* dD, double precision, double m
   P.precision = precision;
   P.boys = e->boys.p;
   P.counter = counter;
+  P.dstride = NOALLOC_CC;
   P.kchunk = 128;  // one ket per thread: small classes still spread over the SMs
   for (int A = 0; A < NPAIRCLASS; ++A)
     for (int B = 0; B <= A; ++B) {
@@ -328,6 +399,49 @@ int direct_jk_noalloc(jk_engine* e, const double* dD, double precision, double m
 using namespace m2;
 
 extern "C" {
+
+int jk_direct_uhf_device(jk_engine* e, const double* dDa, const double* dDb, double precision, double multiplier,
+                         double* dJa, double* dJb, double* dKa, double* dKb, void* stream) {
+  if (!e || !dDa || !dDb || !dJa || !dJb || !dKa || !dKb) return JK_ERR_ARG;
+  if (!(precision >= 0.0)) return set_error(e, JK_ERR_ARG, "jk_direct_uhf: precision must be >= 0");
+  return direct_jk_uhf_device(e, dDa, dDb, precision, multiplier, dJa, dJb, dKa, dKb,
+                              stream ? (cudaStream_t)stream : e->stream);
+}
+
+int jk_direct_uhf(jk_engine* e, const double* Da, const double* Db, double precision, double multiplier, double* Ja,
+                  double* Jb, double* Ka, double* Kb) {
+  if (!e || !Da || !Db || !Ja || !Jb || !Ka || !Kb) return JK_ERR_ARG;
+  const int n = e->obs.n_final;
+  const size_t nn = (size_t)n * n, bytes = sizeof(double) * nn;
+  DevBuf<double> d;
+  cudaError_t st = d.alloc(6 * nn);
+  if (st == cudaSuccess) st = cudaMemcpyAsync(d.p, Da, bytes, cudaMemcpyHostToDevice, e->stream);
+  if (st == cudaSuccess) st = cudaMemcpyAsync(d.p + nn, Db, bytes, cudaMemcpyHostToDevice, e->stream);
+  if (st != cudaSuccess) return check_cuda(e, st, "jk_direct_uhf upload");
+  int rc = jk_direct_uhf_device(e, d.p, d.p + nn, precision, multiplier, d.p + 2 * nn, d.p + 3 * nn, d.p + 4 * nn,
+                                d.p + 5 * nn, nullptr);
+  if (rc) return rc;
+  double* outs[4] = {Ja, Jb, Ka, Kb};
+  for (int k = 0; k < 4 && st == cudaSuccess; ++k)
+    st = cudaMemcpyAsync(outs[k], d.p + (2 + k) * nn, bytes, cudaMemcpyDeviceToHost, e->stream);
+  if (st == cudaSuccess) st = cudaStreamSynchronize(e->stream);
+  return check_cuda(e, st, "jk_direct_uhf download");
+}
+
+int jk_last_class_work(const jk_engine* e, long long* out, int nmax, int* nwritten) {
+  if (!e || !out || !nwritten) return JK_ERR_ARG;
+  *nwritten = 0;
+  if (!e->class_work_valid || !e->class_work.p) return JK_ERR_STATE;
+  std::vector<unsigned long long> h(3 * NPAIRCLASS * NPAIRCLASS);
+  if (cudaMemcpyAsync(h.data(), e->class_work.p, h.size() * sizeof(h[0]), cudaMemcpyDeviceToHost, e->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(e->stream) != cudaSuccess)
+    return JK_ERR_CUDA;
+  const int k = std::min<int>(nmax, (int)h.size());
+  for (int i = 0; i < k; ++i) out[i] = (long long)h[i];
+  *nwritten = k;
+  return JK_OK;
+}
 
 int jk_direct_noalloc(jk_engine* e, const double* dD, double precision, double multiplier, double* dJ, double* dK,
                       void* stream) {

@@ -177,13 +177,15 @@ struct JKParams {
   const double* Dnorm;  // nshell x nshell (final-basis shell-block max norms)
   int nshell;
   const double* Dmax;   // device scalar
-  const double* Dc;     // Cartesian density, nc x nc
+  const double* Dc;     // Cartesian density, nc x nc (NDEN of them, dstride apart)
   int nc;
-  double* Jc;           // raw accumulators
+  double* Jc;           // raw accumulators (NDEN of each, dstride apart)
   double* Kc;
+  size_t dstride;       // elements between consecutive densities / accumulators
   double precision;
   const double* boys;
   unsigned long long* counter;
+  unsigned long long* work;  // NULL or this class pair's [quartets, sum bra primitive pairs, sum primitive quartets]
   int kchunk;
 };
 
@@ -216,7 +218,10 @@ __device__ __forceinline__ void atomic_add_f64(double* a, double v) {
   if (v != 0.0) atomicAdd(a, v);
 }
 
-template <int LA, int LB, int LC, int LD>
+// NDEN densities (1: RHF; 2: the alpha and beta densities of UHF,
+// UnrestrictedFock::formJKdirect, src/fockbuild.cpp:266-362) are digested from
+// the same integrals; the screen uses the norms of their sum.
+template <int LA, int LB, int LC, int LD, int NDEN = 1>
 __global__ void __launch_bounds__(128) k_jk_direct(const JKParams P) {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   constexpr bool BIG = NA * NB * NC * ND > UNROLL_LIMIT;
@@ -236,12 +241,13 @@ __global__ void __launch_bounds__(128) k_jk_direct(const JKParams P) {
   const int a0 = P.sh.coff[a], b0 = P.sh.coff[b];
   const int bp0 = P.bra.prim_off[bra], bnp = P.bra.nprim[bra];
   const int nc = P.nc;
-  const double* __restrict__ Dc = P.Dc;
 
-  double jab[NA * NB];
+  double jab[NDEN][NA * NB];
 #pragma unroll
-  for (int i = 0; i < NA * NB; ++i) jab[i] = 0.0;
-  unsigned long long cnt = 0;
+  for (int dd = 0; dd < NDEN; ++dd)
+#pragma unroll
+    for (int i = 0; i < NA * NB; ++i) jab[dd][i] = 0.0;
+  unsigned long long cnt = 0, wb = 0, wq = 0;
 
   for (int kl = start + threadIdx.x; kl < end; kl += blockDim.x) {
     const int c = P.ket.sa[kl], d = P.ket.sb[kl];
@@ -252,11 +258,18 @@ __global__ void __launch_bounds__(128) k_jk_direct(const JKParams P) {
     dn = fmax(dn, fmax(Dn[b * ns + c], Dn[b * ns + d]));
     if (dn * Qab * Qcd < P.precision) continue;
     ++cnt;
+    wb += bnp;
+    wq += (unsigned long long)bnp * P.ket.nprim[kl];
     double eri[NA * NB * NC * ND];
     quartet_cart<LA, LB, LC, LD>(P.pp, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.pp, P.ket.prim_off[kl], P.ket.nprim[kl],
                                  P.sh.x[c], P.sh.y[c], P.sh.z[c], P.sh.x[d], P.sh.y[d], P.sh.z[d], P.boys, eri);
     const double deg = ((a == b) ? 1.0 : 2.0) * ((c == d) ? 1.0 : 2.0) * ((P.same_class && kl == bra) ? 1.0 : 2.0);
     const int c0 = P.sh.coff[c], d0 = P.sh.coff[d];
+#pragma unroll
+    for (int dd = 0; dd < NDEN; ++dd) {
+    const double* __restrict__ Dc = P.Dc + dd * P.dstride;
+    double* __restrict__ Jd = P.Jc + dd * P.dstride;
+    double* __restrict__ Kd = P.Kc + dd * P.dstride;
     double jcd[NC * ND], kac[NA * NC], kbd[NB * ND], kad[NA * ND], kbc[NB * NC];
 #pragma unroll
     for (int i = 0; i < NC * ND; ++i) jcd[i] = 0.0;
@@ -281,7 +294,7 @@ __global__ void __launch_bounds__(128) k_jk_direct(const JKParams P) {
 #pragma unroll
             for (int id = 0; id < ND; ++id) {
               const double v = eri[((ia * NB + ib) * NC + ic) * ND + id] * deg;
-              jab[ia * NB + ib] += Dc[(size_t)(c0 + ic) * nc + d0 + id] * v;
+              jab[dd][ia * NB + ib] += Dc[(size_t)(c0 + ic) * nc + d0 + id] * v;
               jcd[ic * ND + id] += dab * v;
               kac[ia * NC + ic] += Dc[(size_t)(b0 + ib) * nc + d0 + id] * v;
               kbd[ib * ND + id] += dac * v;
@@ -315,32 +328,46 @@ __global__ void __launch_bounds__(128) k_jk_direct(const JKParams P) {
             kac[ia * NC + ic] += kacs;
             kbc[ib * NC + ic] += kbcs;
           }
-          jab[ia * NB + ib] += jsum;
+          jab[dd][ia * NB + ib] += jsum;
         }
     }
 #pragma unroll
-    for (int i = 0; i < NC * ND; ++i) atomic_add_f64(P.Jc + (size_t)(c0 + i / ND) * nc + d0 + i % ND, jcd[i]);
+    for (int i = 0; i < NC * ND; ++i) atomic_add_f64(Jd + (size_t)(c0 + i / ND) * nc + d0 + i % ND, jcd[i]);
 #pragma unroll
-    for (int i = 0; i < NA * NC; ++i) atomic_add_f64(P.Kc + (size_t)(a0 + i / NC) * nc + c0 + i % NC, kac[i]);
+    for (int i = 0; i < NA * NC; ++i) atomic_add_f64(Kd + (size_t)(a0 + i / NC) * nc + c0 + i % NC, kac[i]);
 #pragma unroll
-    for (int i = 0; i < NB * ND; ++i) atomic_add_f64(P.Kc + (size_t)(b0 + i / ND) * nc + d0 + i % ND, kbd[i]);
+    for (int i = 0; i < NB * ND; ++i) atomic_add_f64(Kd + (size_t)(b0 + i / ND) * nc + d0 + i % ND, kbd[i]);
 #pragma unroll
-    for (int i = 0; i < NA * ND; ++i) atomic_add_f64(P.Kc + (size_t)(a0 + i / ND) * nc + d0 + i % ND, kad[i]);
+    for (int i = 0; i < NA * ND; ++i) atomic_add_f64(Kd + (size_t)(a0 + i / ND) * nc + d0 + i % ND, kad[i]);
 #pragma unroll
-    for (int i = 0; i < NB * NC; ++i) atomic_add_f64(P.Kc + (size_t)(b0 + i / NC) * nc + c0 + i % NC, kbc[i]);
+    for (int i = 0; i < NB * NC; ++i) atomic_add_f64(Kd + (size_t)(b0 + i / NC) * nc + c0 + i % NC, kbc[i]);
+    }  // densities
   }
   // J_ab: the whole block shares the bra pair
   const unsigned lane = threadIdx.x & 31;
 #pragma unroll
-  for (int i = 0; i < NA * NB; ++i) {
-    double v = jab[i];
+  for (int dd = 0; dd < NDEN; ++dd)
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) atomic_add_f64(P.Jc + (size_t)(a0 + i / NB) * nc + b0 + i % NB, v);
+    for (int i = 0; i < NA * NB; ++i) {
+      double v = jab[dd][i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) atomic_add_f64(P.Jc + dd * P.dstride + (size_t)(a0 + i / NB) * nc + b0 + i % NB, v);
+    }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    wb += __shfl_down_sync(0xffffffffu, wb, o);
+    wq += __shfl_down_sync(0xffffffffu, wq, o);
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
-  if (lane == 0 && cnt) atomicAdd(P.counter, cnt);
+  if (lane == 0 && cnt) {
+    atomicAdd(P.counter, cnt);
+    if (P.work) {
+      atomicAdd(P.work, cnt);
+      atomicAdd(P.work + 1, wb);
+      atomicAdd(P.work + 2, wq);
+    }
+  }
 }
 
 // Schwarz bound of each pair of one class: sqrt(max diag (ab|ab)) over the
@@ -405,11 +432,12 @@ struct PairClassDev;
 PairView view(const PairClassDev& c);
 
 // per-translation-unit launchers (jk_cls_*.cu); A, B are pair-class ids
-void launch_jk_bra_s(int A, int B, const JKParams& P, dim3 grid, cudaStream_t s);   // A in {0,1,2}
-void launch_jk_bra_ds(int B, const JKParams& P, dim3 grid, cudaStream_t s);         // A = 3
-void launch_jk_bra_dp(int B, const JKParams& P, dim3 grid, cudaStream_t s);         // A = 4
-void launch_jk_bra_dd_lo(int B, const JKParams& P, dim3 grid, cudaStream_t s);      // A = 5, B < 4
-void launch_jk_bra_dd_hi(int B, const JKParams& P, dim3 grid, cudaStream_t s);      // A = 5, B >= 4
+// nden: densities digested per quartet (1 or 2)
+void launch_jk_bra_s(int A, int B, int nden, const JKParams& P, dim3 grid, cudaStream_t s);   // A in {0,1,2}
+void launch_jk_bra_ds(int B, int nden, const JKParams& P, dim3 grid, cudaStream_t s);         // A = 3
+void launch_jk_bra_dp(int B, int nden, const JKParams& P, dim3 grid, cudaStream_t s);         // A = 4
+void launch_jk_bra_dd_lo(int B, int nden, const JKParams& P, dim3 grid, cudaStream_t s);      // A = 5, B < 4
+void launch_jk_bra_dd_hi(int B, int nden, const JKParams& P, dim3 grid, cudaStream_t s);      // A = 5, B >= 4
 void launch_schwarz_dd(const SchwarzParams& P, dim3 grid, cudaStream_t s);
 
 }  // namespace m2

@@ -20,6 +20,15 @@
 
 namespace m2 {
 
+__global__ void k_add_diag(double* A, const double* d, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) A[(size_t)i * n + i] += d[i];
+}
+static void launch_add_diag(double* A, const double* d, int n, cudaStream_t s) {
+  k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(A, d, n);
+}
+
+
 namespace {
 
 struct Gpu {
@@ -276,16 +285,36 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   if (!syev(S.p, W.p, eps.p)) return set_error(e, JK_ERR_CUDA, "syevd(S)");
   cudaMemcpyAsync(lam.data(), eps.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
+  // lindep > 0: canonical orthogonalisation X = U diag(d) with the directions
+  // of S eigenvalues <= lindep dropped (d = 0) and their Fock diagonal raised
+  // to LINDEP_SHIFT so that they are never occupied; lindep = 0: molecular2's
+  // symmetric S^-1/2 over every direction
+  constexpr double LINDEP_SHIFT = 1e4;
+  std::vector<double> shift(n, 0.0);
+  int ndrop = 0;
   for (int i = 0; i < n; ++i) {
-    if (!(lam[i] > 0.0)) return set_error(e, JK_ERR_ARG, "overlap matrix is not positive definite");
-    lam[i] = 1.0 / std::sqrt(lam[i]);
+    if (!(lam[i] > 0.0) && !(o->lindep > 0.0))
+      return set_error(e, JK_ERR_ARG, "overlap matrix is not positive definite");
+    if (o->lindep > 0.0 && lam[i] <= o->lindep) {
+      lam[i] = 0.0;
+      shift[i] = LINDEP_SHIFT;
+      ++ndrop;
+    } else {
+      lam[i] = 1.0 / std::sqrt(lam[i]);
+    }
   }
+  if (nocc > n - ndrop) return set_error(e, JK_ERR_ARG, "scf: lindep leaves fewer orbitals than nocc");
+  DevBuf<double> dshift;
+  if (ndrop > 0 && (st = dshift.upload(shift, s)) != cudaSuccess) return check_cuda(e, st, "scf lindep shift");
   g.copy(W.p, t1.p, nn);
   {
     DevBuf<double> dl;
     dl.upload(lam, s);
     cublasDdgmm(e->cublas, CUBLAS_SIDE_RIGHT, n, n, t1.p, n, dl.p, 1, t1.p, n);  // U diag
-    g.mm(false, true, t1.p, W.p, X.p);                                              // (U diag) U^T
+    if (o->lindep > 0.0)
+      g.copy(t1.p, X.p, nn);              // canonical: U diag
+    else
+      g.mm(false, true, t1.p, W.p, X.p);  // symmetric: (U diag) U^T
     cudaStreamSynchronize(s);
   }
   double jk_ms = 0.0, diag_ms = 0.0;
@@ -306,6 +335,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   const bool corrected = mixed && refresh_every > 0;
   int fp64_after_switch = 0;
   bool switched = !mixed, have_delta = false;
+  int build_kind = 0;  // of the last Fock build (trace)
   int since_refresh = 0, refreshes = 0;
   double dd_hist[3] = {1e300, 1e300, 1e300};
   cudaEvent_t ev_a, ev_b;
@@ -331,9 +361,10 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   diis.use = o->diis != 0;
   if ((st = focks.init(MAX, nn)) != cudaSuccess || (st = diis.errs.init(MAX, nn)) != cudaSuccess)
     return check_cuda(e, st, "scf DIIS history");
-  auto transform = [&](const double* Fa) {  // Fm = X^T F X
+  auto transform = [&](const double* Fa) {  // Fm = X^T F X (+ the shift of dropped directions)
     g.mm(false, false, Fa, X.p, t1.p);
     g.mm(true, false, X.p, t1.p, Fm.p);
+    if (ndrop > 0) launch_add_diag(Fm.p, dshift.p, n, s);
   };
   bool have_W = false;  // W holds the eigenvectors of the previous Fm
   auto diagonalise = [&]() -> bool {
@@ -466,8 +497,10 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
       int rc2 = JK_OK;
       if (corrected && switched) align();
       if (!switched) {
+        build_kind = 1;
         rc2 = jk(nullptr, t2.p, 1);
       } else if (corrected && (!have_delta || since_refresh >= refresh_every)) {
+        build_kind = 3;
         if ((rc2 = jk(nullptr, Delta.p, 1))) return rc2;
         if ((rc2 = jk(nullptr, t2.p, 0))) return rc2;
         g.scal(-1.0, Delta.p, nn);
@@ -480,11 +513,13 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
         diis.reset();
         fock_iter = 0;
       } else if (corrected) {
+        build_kind = 2;
         if ((rc2 = jk(nullptr, t2.p, 1))) return rc2;
         g.axpy(1.0, Delta.p, t2.p, nn);
         ++corrected_builds;
         ++since_refresh;
       } else {
+        build_kind = 0;
         rc2 = jk(nullptr, t2.p, 0);
         if (mixed) ++fp64_after_switch;
       }
@@ -566,6 +601,14 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     // a mixed run converges only on FP64 (or FP64-corrected) builds
     const bool precise = !mixed || (corrected ? (have_delta && since_refresh >= 2) : fp64_after_switch >= 2);
     converged = dd < o->densconverge && delta < o->enconverge && precise;
+    if (o->out_trace && it < o->maxiter) {
+      double* tr = o->out_trace + (size_t)5 * it;
+      tr[0] = energy;
+      tr[1] = dd;
+      tr[2] = rms_error;
+      tr[3] = build_kind;
+      tr[4] = g.nrm2(D.p, nn);
+    }
     ++it;
   }
   if (mixed) {
@@ -591,6 +634,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   r->last_delta_d = dd;
   r->mixed_builds = mixed_builds;
   r->diag_ms = diag_ms;
+  r->lindep_dropped = ndrop;
   if (o->out_density) cudaMemcpy(o->out_density, D.p, nn * sizeof(double), cudaMemcpyDeviceToHost);
   if (o->out_coeffs) cudaMemcpy(o->out_coeffs, C.p, nn * sizeof(double), cudaMemcpyDeviceToHost);
   if (o->out_eps) cudaMemcpy(o->out_eps, eps.p, n * sizeof(double), cudaMemcpyDeviceToHost);

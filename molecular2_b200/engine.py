@@ -37,7 +37,12 @@ SIGNATURES = {
     "jk_direct": (_I, [_P, _P, _D, _D, _P, _P]),
     "jk_direct_device": (_I, [_P, _P, _D, _D, _P, _P, _P]),
     "jk_direct_noalloc": (_I, [_P, _P, _D, _D, _P, _P, _P]),
+    "jk_direct_uhf": (_I, [_P, _P, _P, _D, _D, _P, _P, _P, _P]),
+    "jk_direct_uhf_device": (_I, [_P, _P, _P, _D, _D, _P, _P, _P, _P, _P]),
+    "jk_df_uhf": (_I, [_P, _P, _I, _P, _I, _I, _D, _P, _P, _P, _P]),
+    "jk_df_uhf_device": (_I, [_P, _P, _I, _P, _I, _I, _D, _P, _P, _P, _P, _P]),
     "jk_last_quartets": (ctypes.c_longlong, [_P]),
+    "jk_last_class_work": (_I, [_P, _P, _I, ctypes.POINTER(_I)]),
     "jk_eri3": (_I, [_P, _P]),
     "jk_eri2": (_I, [_P, _P]),
     "jk_df_setup": (_I, [_P]),
@@ -63,13 +68,14 @@ class SCFOptions(ctypes.Structure):
                 ("eig_mode", _I),
                 ("maxiter", _I), ("maxdiis", _I), ("diis", _I),
                 ("precision", _D), ("enconverge", _D), ("densconverge", _D), ("enuc", _D),
-                ("guess_fock", _P), ("out_density", _P), ("out_coeffs", _P), ("out_eps", _P)]
+                ("guess_fock", _P), ("out_density", _P), ("out_coeffs", _P), ("out_eps", _P),
+                ("out_trace", _P), ("lindep", _D)]
 
 
 class SCFResult(ctypes.Structure):
     _fields_ = [("energy", _D), ("iterations", _I), ("converged", _I), ("jk_builds", _I), ("jk_ms", _D),
                 ("total_ms", _D), ("last_delta_e", _D), ("last_delta_d", _D), ("mixed_builds", _I),
-                ("diag_ms", _D)]
+                ("diag_ms", _D), ("lindep_dropped", _I)]
 
 
 class JKError(RuntimeError):
@@ -160,6 +166,14 @@ class IntegralEngine:
 
     compute_schwarz_ints = getPrescreen
 
+    def last_class_work(self):
+        """(6 x 6 x 3) array over (bra class, ket class) of the last direct build:
+        quartets, bra primitive pairs, primitive quartets (classes ss, ps, pp, ds, dp, dd)."""
+        out = np.zeros(108, dtype=np.int64)
+        nw = ctypes.c_int(0)
+        self._check(self.lib.jk_last_class_work(self.h, _p(out), 108, ctypes.byref(nw)))
+        return out.reshape(6, 6, 3)
+
     def last_quartets(self):
         return int(self.lib.jk_last_quartets(self.h))
 
@@ -177,6 +191,26 @@ class IntegralEngine:
         self._check(self.lib.jk_direct_device(self.h, ctypes.c_void_p(dD), precision, multiplier,
                                               ctypes.c_void_p(dJ), ctypes.c_void_p(dK),
                                               ctypes.c_void_p(stream) if stream else None))
+
+    def jk_direct_uhf(self, Da, Db, precision=1e-12, multiplier=1.0):
+        """UnrestrictedFock::formJKdirect (src/fockbuild.cpp:266-362): (Ja, Jb, Ka, Kb)."""
+        n = self.n
+        Da = np.asfortranarray(Da, dtype=np.float64)
+        Db = np.asfortranarray(Db, dtype=np.float64)
+        out = [np.zeros((n, n), order="F") for _ in range(4)]
+        self._check(self.lib.jk_direct_uhf(self.h, _p(Da), _p(Db), precision, multiplier, *[_p(o) for o in out]))
+        return tuple(out)
+
+    def jk_df_uhf(self, Ca, Cb, prec_mode=0, multiplier=1.0):
+        """UnrestrictedFock::formJKdf (src/fockbuild.cpp:365-372): (Ja, Jb, Ka, Kb)
+        w.r.t. Ca Ca^T and Cb Cb^T."""
+        n = self.n
+        Ca = np.asfortranarray(Ca, dtype=np.float64).reshape(n, -1)
+        Cb = np.asfortranarray(Cb, dtype=np.float64).reshape(n, -1)
+        out = [np.zeros((n, n), order="F") for _ in range(4)]
+        self._check(self.lib.jk_df_uhf(self.h, _p(Ca), Ca.shape[1], _p(Cb), Cb.shape[1], prec_mode, multiplier,
+                                       *[_p(o) for o in out]))
+        return tuple(out)
 
     # -- density fitting -----------------------------------------------------
     def compute_eris_3index(self):
@@ -292,7 +326,7 @@ class IntegralEngine:
 
     def scf_rhf(self, nocc, enuc, df=False, prec_mode=0, maxiter=40, maxdiis=8, diis=True, precision=1e-12,
                 enconverge=1e-7, densconverge=1e-4, guess_fock=None, want=False, mixed_switch=1e-3, eig_mode=0,
-                mixed_refresh=0, guess="core"):
+                mixed_refresh=0, guess="core", lindep=0.0):
         """SCF::rhf on the device; returns (SCFResult, extras dict).  guess is
         "core" (core Hamiltonian) or "soad" (SOAD Fock, the reference default);
         an explicit guess_fock overrides it."""
@@ -305,12 +339,15 @@ class IntegralEngine:
         o.nocc, o.df, o.prec_mode, o.maxiter, o.maxdiis, o.diis = nocc, int(df), prec_mode, maxiter, maxdiis, int(diis)
         o.mixed_switch, o.eig_mode, o.mixed_refresh = mixed_switch, eig_mode, mixed_refresh
         o.precision, o.enconverge, o.densconverge, o.enuc = precision, enconverge, densconverge, enuc
+        o.lindep = lindep
         keep = []
         if guess_fock is not None:
             gf = np.asfortranarray(guess_fock, dtype=np.float64)
             keep.append(gf)
             o.guess_fock = gf.ctypes.data
         extras = {}
+        trace = np.zeros((max(1, maxiter), 5))
+        o.out_trace = trace.ctypes.data
         if want:
             extras = {"D": np.zeros((n, n), order="F"), "C": np.zeros((n, n), order="F"), "eps": np.zeros(n)}
             o.out_density, o.out_coeffs, o.out_eps = (extras[k].ctypes.data for k in ("D", "C", "eps"))
@@ -318,6 +355,7 @@ class IntegralEngine:
         rc = self.lib.jk_scf_rhf(self.h, ctypes.byref(o), ctypes.byref(r))
         if rc not in (0, 6):
             self._check(rc)
+        extras["trace"] = trace[:max(0, min(r.iterations, maxiter))]
         return r, extras
 
 

@@ -48,6 +48,7 @@ def lib():
             "orc_shellblock_norm": (None, [P, P, P]),
             "orc_jk_direct": (ctypes.c_long, [P, P, P, d, d, P, P, i]),
             "orc_jk_direct_rows": (ctypes.c_long, [P, P, P, d, i, i, P, P]),
+            "orc_jk_direct_uhf": (ctypes.c_long, [P, P, P, P, d, d, P, P, P, P, i]),
             "orc_fock_general": (None, [P, P, P, i, P]),
             "orc_eri3": (None, [P, P, P]),
             "orc_eri2": (None, [P, P]),
@@ -138,6 +139,18 @@ def jk_direct(basis, D, Q=None, precision=1e-12, multiplier=1.0, nthreads=None):
     nt = nthreads or os.cpu_count() or 1
     cnt = lib().orc_jk_direct(_bp(basis), _p(Qc), _p(D), precision, multiplier, _p(J), _p(K), nt)
     return J, K, cnt
+
+
+def jk_direct_uhf(basis, Da, Db, Q=None, precision=1e-12, multiplier=1.0, nthreads=None):
+    """UnrestrictedFock::formJKdirect: (Ja, Jb, Ka, Kb, quartets)."""
+    n = basis.nbf
+    Qc = None if Q is None else np.ascontiguousarray(Q, dtype=np.float64)
+    Da, Db = F(Da), F(Db)
+    out = [np.zeros((n, n), order="F") for _ in range(4)]
+    nt = nthreads or os.cpu_count() or 1
+    cnt = lib().orc_jk_direct_uhf(_bp(basis), _p(Qc) if Qc is not None else None, _p(Da), _p(Db), precision,
+                                  multiplier, *[_p(o) for o in out], nt)
+    return (*out, cnt)
 
 
 def jk_direct_rows(basis, D, Q, precision, s1_begin, s1_end):

@@ -830,6 +830,83 @@ long orc_jk_direct(const orc_basis* b, const double* Q, const double* D, double 
   return total;
 }
 
+// UnrestrictedFock::formJKdirect (src/fockbuild.cpp:266-362): the loop of
+// formJKdirect with the screen built from the shell-block norms of Da + Db and
+// every integral batch digested into both spin densities.  Outputs are w.r.t.
+// each full spin density, times multiplier.  Returns the quartet count.
+long orc_jk_direct_uhf(const orc_basis* b, const double* Q, const double* Da, const double* Db, double precision,
+                       double multiplier, double* Ja, double* Jb, double* Ka, double* Kb, int nthreads) {
+  Basis B = make_basis(b);
+  const int ns = (int)B.sh.size(), n = B.n;
+  const size_t nn = (size_t)n * n;
+  const bool screen = Q != nullptr;
+  std::vector<double> Dt(nn);
+  for (size_t i = 0; i < nn; ++i) Dt[i] = Da[i] + Db[i];
+  auto Dn = shellblock_norm(B, Dt.data());
+  if (nthreads < 1) nthreads = 1;
+  // per thread: Ja, Jb, Ka, Kb accumulators
+  std::vector<std::vector<double>> acc(nthreads, std::vector<double>(4 * nn, 0.0));
+  std::vector<long> cnt(nthreads, 0);
+  auto dn = [&](int a, int c) { return Dn[(size_t)a * ns + c]; };
+  parallel_for(ns, nthreads, [&](int s1, int t) {
+    std::vector<double> buf;
+    double* A = acc[t].data();
+    for (int s2 = 0; s2 <= s1; ++s2) {
+      const double Dnorm12 = screen ? dn(s1, s2) : 0.0;
+      for (int s3 = 0; s3 <= s1; ++s3) {
+        const double Dnorm123 = screen ? std::max(dn(s1, s3), std::max(dn(s2, s3), Dnorm12)) : 0.0;
+        const int s4_max = (s1 == s3) ? s2 : s3;
+        for (int s4 = 0; s4 <= s4_max; ++s4) {
+          const double Dnorm1234 =
+              screen ? std::max(dn(s1, s4), std::max(dn(s2, s4), std::max(dn(s3, s4), Dnorm123))) : 0.0;
+          if (screen && Dnorm1234 * Q[(size_t)s1 * ns + s2] * Q[(size_t)s3 * ns + s4] < precision) continue;
+          const double deg = ((s1 == s2) ? 1.0 : 2.0) * ((s3 == s4) ? 1.0 : 2.0) *
+                             ((s1 == s3) ? (s2 == s4 ? 1.0 : 2.0) : 2.0);
+          shell_eri(B.sh[s1], B.sh[s2], B.sh[s3], B.sh[s4], buf);
+          ++cnt[t];
+          const int n1 = B.sh[s1].nbf(), n2 = B.sh[s2].nbf(), n3 = B.sh[s3].nbf(), n4 = B.sh[s4].nbf();
+          for (int spin = 0; spin < 2; ++spin) {
+            const double* D = spin ? Db : Da;
+            double* Jm = A + spin * nn;
+            double* Km = A + (2 + spin) * nn;
+            auto Dm = [&](int i, int j) { return D[(size_t)j * n + i]; };
+            for (int f1 = 0, f = 0; f1 < n1; ++f1) {
+              const int b1 = B.off[s1] + f1;
+              for (int f2 = 0; f2 < n2; ++f2) {
+                const int b2 = B.off[s2] + f2;
+                for (int f3 = 0; f3 < n3; ++f3) {
+                  const int b3 = B.off[s3] + f3;
+                  for (int f4 = 0; f4 < n4; ++f4, ++f) {
+                    const int b4 = B.off[s4] + f4;
+                    const double v = multiplier * buf[f] * deg;
+                    Jm[(size_t)b2 * n + b1] += Dm(b3, b4) * v;
+                    Jm[(size_t)b4 * n + b3] += Dm(b1, b2) * v;
+                    Km[(size_t)b3 * n + b1] += 0.5 * Dm(b2, b4) * v;
+                    Km[(size_t)b4 * n + b2] += 0.5 * Dm(b1, b3) * v;
+                    Km[(size_t)b4 * n + b1] += 0.5 * Dm(b2, b3) * v;
+                    Km[(size_t)b3 * n + b2] += 0.5 * Dm(b1, b4) * v;
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+  });
+  long total = 0;
+  for (int t = 0; t < nthreads; ++t) total += cnt[t];
+  for (int t = 1; t < nthreads; ++t)
+    for (size_t i = 0; i < 4 * nn; ++i) acc[0][i] += acc[t][i];
+  double* outs[4] = {Ja, Jb, Ka, Kb};
+  for (int k = 0; k < 4; ++k) {
+    const double* X = acc[0].data() + k * nn;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) outs[k][(size_t)j * n + i] = 0.25 * (X[(size_t)j * n + i] + X[(size_t)i * n + j]);
+  }
+  return total;
+}
+
 // Time-bounded variant for the CPU baseline: runs the same loop for s1 in
 // [s1_begin, s1_end) only and returns the number of quartets computed.
 long orc_jk_direct_rows(const orc_basis* b, const double* Q, const double* D, double precision, int s1_begin,
