@@ -32,7 +32,9 @@ oracle's restatement of compute_2body_fock_df's naive loops (molecular2
 itself needs libint2/Eigen and cannot be built here; its packed FP64 B for
 this system would be 264 GB), on a bounded sample of the fitting functions,
 extrapolated linearly in naux.
---profile runs only the set-up and the timed builds (for ncu launch lists).
+--profile runs only the set-up and the timed builds (for ncu launch lists);
+--precision fp64 times FP64 builds instead of mixed ones; --workload water16aug
+is the small case of the tiled kernels used for ncu captures.
 With --gpus N > 1 every rank runs its own replica of the workload (the
 north-star measurement is single-GPU).
 """
@@ -58,6 +60,9 @@ WORKLOADS = {
                     obs="aug-cc-pvdz", aux="avdz-jkfit", storage="tiled"),
     "water16": dict(label="(H2O)16 RHF/cc-pVDZ + VDZ-JKFIT", k=16, box=9.0, seed=16,
                     obs="cc-pvdz", aux="vdz-jkfit", storage="unpacked"),
+    # the small case of the tiled kernels for ncu captures (3.3 GB of split B)
+    "water16aug": dict(label="(H2O)16 RHF/aug-cc-pVDZ + AVDZ-JKFIT", k=16, box=9.0, seed=16,
+                       obs="aug-cc-pvdz", aux="avdz-jkfit", storage="tiled"),
 }
 _CACHE = {}
 
@@ -428,8 +433,10 @@ def run_ours(args, rank, world, local):
         dK = torch.empty((n, n), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
 
+    mode = 0 if args.precision == "fp64" else 1
+
     def step():
-        eng.jk_df_device(dC.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), 1, stream=sh)
+        eng.jk_df_device(dC.data_ptr(), nocc, dJ.data_ptr(), dK.data_ptr(), mode, stream=sh)
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -549,6 +556,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="water64", choices=sorted(WORKLOADS))
     ap.add_argument("--profile", action="store_true")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="precision of the timed builds (the SCF comparison runs both)")
     ap.add_argument("--clock-dir", default=None, help="where the nvidia-smi clock samples go (default: a temp dir)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the smaller workloads")

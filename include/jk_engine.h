@@ -159,6 +159,15 @@ int jk_df_uhf(jk_engine* e, const double* Ca, int na, const double* Cb, int nb, 
 int jk_df_uhf_device(jk_engine* e, const double* dCa, int na, const double* dCb, int nb, int prec_mode,
                      double multiplier, double* dJa, double* dJb, double* dKa, double* dKb, void* stream);
 
+/* Density-fitted MP2 correlation energy for the canonical orbitals C (n x nmo
+ * column-major, host) with orbital energies eps (nmo): the nfrozen lowest of
+ * the nocc occupied orbitals are frozen, the nmo - nocc above them are the
+ * virtuals.  (ia|jb) comes from the fitted tensor of jk_df_setup (unpacked
+ * storage; run first if needed), E = sum (ia|jb)[2(ia|jb) - (ib|ja)] /
+ * (e_i + e_j - e_a - e_b) in FP64.  Replaces MP2::dfmp2 (src/mp2.cpp:477-583),
+ * which inverts (P|Q) explicitly where this uses its Cholesky factor. */
+int jk_df_mp2(jk_engine* e, const double* C, const double* eps, int nmo, int nocc, int nfrozen, double* emp2);
+
 /* Layout of the fitted tensor, chosen before jk_df_setup (molecular2 keeps one
  * packed FP64 (n(n+1)/2) x naux matrix, src/fockbuild.cpp:598-619, which
  * stops fitting in device memory near n = 2600, naux = 9600):
@@ -220,7 +229,11 @@ typedef struct jk_scf_options {
   int df;                  /* 0 = integral-direct J/K, 1 = density-fitted */
   int prec_mode;           /* DF only: 0 = FP64; 1 = split-BF16 tensor-core builds while
                               ||D - D_old||_F >= mixed_switch and still falling, FP64
-                              builds to convergence after that */
+                              builds to convergence after that (or, with mixed_refresh,
+                              corrected mixed builds); 2 = the same mixed phase, then an FP64
+                              anchor build G64(D_ref) and mixed builds of the low-rank change
+                              D - D_ref only (error proportional to ||D - D_ref||), with a second
+                              anchor once ||D - D_old||_F < 100 densconverge */
   double mixed_switch;     /* default 1e-3; the switch also happens when ||dD|| stalls */
   int mixed_refresh;       /* 0 (default): FP64 builds after the switch.  k > 0: mixed builds
                               plus the correction G64 - Gmixed refreshed every k iterations,
@@ -240,7 +253,8 @@ typedef struct jk_scf_options {
   double* out_eps;         /* optional host n */
   double* out_trace;       /* optional host maxiter x 5, per iteration: energy, ||D - D_old||_F, rms of the
                               DIIS error, build kind (0 FP64, 1 mixed, 2 mixed + correction, 3 correction
-                              refresh: mixed and FP64 builds), ||D||_F */
+                              refresh: mixed and FP64 builds, 4 FP64 anchor + mixed build of D - D_ref),
+                              ||D||_F */
   double lindep;           /* 0 (default): symmetric S^-1/2 over all directions as molecular2
                               (src/fock.cpp:124-142); > 0: canonical orthogonalisation dropping the
                               directions whose overlap eigenvalue is <= lindep */

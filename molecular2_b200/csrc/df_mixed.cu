@@ -538,18 +538,24 @@ int df_mixed_prepare(jk_engine* e, int nocc) {
     if (st != cudaSuccess) return check_cuda(e, st, "split B");
     m.ldb = ldb;
     m.NP = 0;
+    m.NP_cap = 0;
     m.ready = true;
   }
   if (m.NP != NP) {
-    st = m.Ch.alloc((size_t)NP * ldb);
-    if (st == cudaSuccess) st = m.Cl.alloc((size_t)NP * ldb);
-    if (st == cudaSuccess) st = m.Xh.alloc((size_t)n * naux * NP);
-    if (st == cudaSuccess) st = m.Xl.alloc((size_t)n * naux * NP);
-    if (st == cudaSuccess) st = m.Kt.alloc((size_t)n * n);
-    if (st == cudaSuccess) st = m.err.alloc(1);
-    if (st == cudaSuccess) st = d.gamma.alloc(naux);
-    if (st != cudaSuccess) return check_cuda(e, st, "mixed scratch allocation");
-    cudaMemsetAsync(m.err.p, 0, sizeof(int), s);
+    // scratch sized for the largest occupied count so far; smaller counts
+    // reuse it with tensor maps for their own row length
+    if (NP > m.NP_cap) {
+      st = m.Ch.alloc((size_t)NP * ldb);
+      if (st == cudaSuccess) st = m.Cl.alloc((size_t)NP * ldb);
+      if (st == cudaSuccess) st = m.Xh.alloc((size_t)n * naux * NP);
+      if (st == cudaSuccess) st = m.Xl.alloc((size_t)n * naux * NP);
+      if (st == cudaSuccess) st = m.Kt.alloc((size_t)n * n);
+      if (st == cudaSuccess) st = m.err.alloc(1);
+      if (st == cudaSuccess) st = d.gamma.alloc(naux);
+      if (st != cudaSuccess) return check_cuda(e, st, "mixed scratch allocation");
+      cudaMemsetAsync(m.err.p, 0, sizeof(int), s);
+      m.NP_cap = NP;
+    }
     bool ok = make_map(&m.maps[0], m.Bh.p, ldb, (uint64_t)n * naux, BK, BM) &&
               make_map(&m.maps[1], m.Bl.p, ldb, (uint64_t)n * naux, BK, BM) &&
               make_map(&m.maps[2], m.Ch.p, ldb, NP, BK, NP) && make_map(&m.maps[3], m.Cl.p, ldb, NP, BK, NP) &&

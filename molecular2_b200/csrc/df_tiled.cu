@@ -565,52 +565,62 @@ int df_tiled_setup(jk_engine* e) {
   return JK_OK;
 }
 
+// Scratch of the mixed build, sized for the largest occupied count seen so far
+// (a smaller count reuses it with tensor maps for its own row length, so the
+// varying column counts of incremental builds allocate nothing).
 static int tiled_mixed_prepare(jk_engine* e, int nocc) {
   TiledDF& T = e->tiled;
   const int naux = e->aux.n_final, n = e->obs.n_final;
   const int nhalf = (nocc + SN - 1) / SN;
   const int NPX = nhalf * SN;
-  if (T.NPX == NPX && T.nocc == nocc && T.Xh.p) return JK_OK;
-  T.Ch.reset();
-  T.Cl.reset();
-  T.Xh.reset();
-  T.Xl.reset();
-  cudaError_t st = T.Ch.alloc((size_t)NPX * T.npad);
-  if (st == cudaSuccess) st = T.Cl.alloc((size_t)NPX * T.npad);
-  if (st == cudaSuccess) st = T.Kt.alloc((size_t)n * n);
-  if (st == cudaSuccess) st = T.err.alloc(1);
-  if (st == cudaSuccess) st = e->df.gamma.alloc(naux);
-  if (st != cudaSuccess) return check_cuda(e, st, "tiled mixed scratch");
-  // X block: as many fitted functions as fit in a quarter of the free memory (at most all)
-  size_t fr = 0, tt = 0;
-  cudaMemGetInfo(&fr, &tt);
-  const double per_k = 4.0 * T.npad * NPX;  // hi + lo BF16
-  int w = (int)std::min<double>(naux, std::max(64.0, 0.25 * fr / per_k));
-  if (T.waux_max > 0) w = std::min(w, T.waux_max);
-  w = std::max(1, std::min(naux, w));
-  // X rows are padded to an even number of fitted functions, so that a row
-  // is a whole number of 64-wide k blocks (NPX is a multiple of 160)
-  for (;; w = w / 2) {
-    const int ws = w + (w & 1);
-    st = T.Xh.alloc((size_t)T.npad * ws * NPX);
-    if (st == cudaSuccess) st = T.Xl.alloc((size_t)T.npad * ws * NPX);
-    if (st == cudaSuccess) break;
+  cudaError_t st;
+  if (!T.Xh.p || NPX > T.NPX_cap) {
+    T.Ch.reset();
+    T.Cl.reset();
     T.Xh.reset();
     T.Xl.reset();
-    cudaGetLastError();
-    if (w <= 16) return check_cuda(e, st, "tiled mixed X block");
+    st = T.Ch.alloc((size_t)NPX * T.npad);
+    if (st == cudaSuccess) st = T.Cl.alloc((size_t)NPX * T.npad);
+    if (st == cudaSuccess) st = T.Kt.alloc((size_t)n * n);
+    if (st == cudaSuccess) st = T.err.alloc(1);
+    if (st == cudaSuccess) st = e->df.gamma.alloc(naux);
+    if (st != cudaSuccess) return check_cuda(e, st, "tiled mixed scratch");
+    // X block: as many fitted functions as fit in a quarter of the free memory (at most all)
+    size_t fr = 0, tt = 0;
+    cudaMemGetInfo(&fr, &tt);
+    const double per_k = 4.0 * T.npad * NPX;  // hi + lo BF16
+    int w = (int)std::min<double>(naux, std::max(64.0, 0.25 * fr / per_k));
+    if (T.waux_max > 0) w = std::min(w, T.waux_max);
+    w = std::max(1, std::min(naux, w));
+    // X rows are padded to an even number of fitted functions, so that a row
+    // is a whole number of 64-wide k blocks (NPX is a multiple of 160)
+    for (;; w = w / 2) {
+      const int ws = w + (w & 1);
+      st = T.Xh.alloc((size_t)T.npad * ws * NPX);
+      if (st == cudaSuccess) st = T.Xl.alloc((size_t)T.npad * ws * NPX);
+      if (st == cudaSuccess) break;
+      T.Xh.reset();
+      T.Xl.reset();
+      cudaGetLastError();
+      if (w <= 16) return check_cuda(e, st, "tiled mixed X block");
+    }
+    T.waux = w;
+    T.wstride = w + (w & 1);
+    T.NPX_cap = NPX;
+    T.NPX = 0;
+    cudaMemsetAsync(T.err.p, 0, sizeof(int), e->stream);
+    const uint64_t brows = (uint64_t)naux * T.npt * TB;
+    const bool ok = make_map(&T.maps[0], T.Bh.p, TB, brows, SBK, TB) && make_map(&T.maps[1], T.Bl.p, TB, brows, SBK, TB) &&
+                    make_map(&T.maps[2], T.Bh.p, TB, brows, SBK, SBK) && make_map(&T.maps[3], T.Bl.p, TB, brows, SBK, SBK);
+    if (!ok) return set_error(e, JK_ERR_CUDA, "cuTensorMapEncodeTiled failed (tiled DF)");
   }
-  T.waux = w;
-  T.wstride = w + (w & 1);
-  cudaMemsetAsync(T.err.p, 0, sizeof(int), e->stream);
-  const uint64_t brows = (uint64_t)naux * T.npt * TB;
-  bool ok = make_map(&T.maps[0], T.Bh.p, TB, brows, SBK, TB) && make_map(&T.maps[1], T.Bl.p, TB, brows, SBK, TB) &&
-            make_map(&T.maps[2], T.Bh.p, TB, brows, SBK, SBK) && make_map(&T.maps[3], T.Bl.p, TB, brows, SBK, SBK) &&
-            make_map(&T.maps[4], T.Ch.p, T.npad, NPX, SBK, SN) && make_map(&T.maps[5], T.Cl.p, T.npad, NPX, SBK, SN) &&
-            make_map(&T.maps[6], T.Xh.p, (uint64_t)T.wstride * NPX, T.npad, SBK, TB) &&
-            make_map(&T.maps[7], T.Xl.p, (uint64_t)T.wstride * NPX, T.npad, SBK, TB);
-  if (!ok) return set_error(e, JK_ERR_CUDA, "cuTensorMapEncodeTiled failed (tiled DF)");
-  T.NPX = NPX;
+  if (T.NPX != NPX) {
+    const bool ok = make_map(&T.maps[4], T.Ch.p, T.npad, NPX, SBK, SN) && make_map(&T.maps[5], T.Cl.p, T.npad, NPX, SBK, SN) &&
+                    make_map(&T.maps[6], T.Xh.p, (uint64_t)T.wstride * NPX, T.npad, SBK, TB) &&
+                    make_map(&T.maps[7], T.Xl.p, (uint64_t)T.wstride * NPX, T.npad, SBK, TB);
+    if (!ok) return set_error(e, JK_ERR_CUDA, "cuTensorMapEncodeTiled failed (tiled DF)");
+    T.NPX = NPX;
+  }
   T.nocc = nocc;
   return JK_OK;
 }
@@ -954,7 +964,8 @@ extern "C" int jk_df_set_tiled_blocks(jk_engine* e, int waux_max, int oc_max) {
   if (waux_max < 0 || oc_max < 0) return set_error(e, JK_ERR_ARG, "jk_df_set_tiled_blocks: negative cap");
   e->tiled.waux_max = waux_max;
   e->tiled.oc_max = oc_max;
-  e->tiled.NPX = 0;  // re-plan the mixed scratch on the next build
+  e->tiled.NPX_cap = 0;  // re-plan the mixed scratch on the next build
+  e->tiled.NPX = 0;
   return JK_OK;
 }
 

@@ -95,6 +95,7 @@ struct MixedState {
   bool ready = false;
   int ldb = 0;                       // padded row length of Bh/Bl (multiple of 64)
   int NP = 0;                        // nocc padded to a multiple of 16
+  int NP_cap = 0;                    // NP the scratch below was allocated for
   DevBuf<__nv_bfloat16> Bh, Bl;      // [x][K][y], ld = ldb
   DevBuf<__nv_bfloat16> Ch, Cl;      // [i][y] (NP x ldb)
   DevBuf<__nv_bfloat16> Xh, Xl;      // [x][K][i] (n x naux*NP)
@@ -117,6 +118,7 @@ struct TiledDF {
   // mixed-build scratch
   int NPX = 0, waux = 0, nocc = 0;   // X row length per K (nhalf * 160), aux block, occupied count
   int wstride = 0;                   // X row stride in fitted functions (waux rounded up to even)
+  int NPX_cap = 0;                   // NPX the mixed scratch was allocated for
   int waux_max = 0, oc_max = 0;      // caps on the aux block and the FP64 occupied slice (0: memory decides)
   DevBuf<__nv_bfloat16> Ch, Cl;      // [i][y], NPX x npad
   DevBuf<__nv_bfloat16> Xh, Xl;      // [x][K_local][i], npad x waux x NPX

@@ -24,6 +24,14 @@ __global__ void k_add_diag(double* A, const double* d, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) A[(size_t)i * n + i] += d[i];
 }
+__global__ void k_scale_columns(const double* __restrict__ U, int n, int r, const double* __restrict__ sc,
+                                double* __restrict__ out) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < (size_t)n * r) out[idx] = U[idx] * sc[idx / n];
+}
+static void launch_scale_columns(const double* U, int n, int r, const double* sc, double* out, cudaStream_t s) {
+  k_scale_columns<<<(unsigned)(((size_t)n * r + 255) / 256), 256, 0, s>>>(U, n, r, sc, out);
+}
 static void launch_add_diag(double* A, const double* d, int n, cudaStream_t s) {
   k_add_diag<<<(n + 255) / 256, 256, 0, s>>>(A, d, n);
 }
@@ -240,6 +248,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   Gpu g{e, s, n};
   DevBuf<double> S, T, V, H, X, F, Fm, Finc, D, Dd, Dold, C, W, Wt, eps, J, K, t1, t2, err, work, Delta;
   DevBuf<double> Cal, Cprev, Um, Vm, Wm;  // orbital alignment of the mixed phase
+  DevBuf<double> Dref, Gref, Ud, Cpm, lamd;  // FP64 anchor and low-rank density change (prec_mode 2)
   DevBuf<int> info;
   cudaError_t st = cudaSuccess;
   for (auto* b : {&S, &T, &V, &H, &X, &F, &Fm, &Finc, &D, &Dd, &Dold, &C, &W, &Wt, &J, &K, &t1, &t2, &err, &Delta,
@@ -247,6 +256,11 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     if (st == cudaSuccess) st = b->alloc(nn);
   if (st == cudaSuccess) st = eps.alloc(n);
   if (st == cudaSuccess) st = info.alloc(1);
+  if (st == cudaSuccess && o->df && o->prec_mode == 2) {
+    for (auto* b : {&Dref, &Gref, &Ud, &Cpm})
+      if (st == cudaSuccess) st = b->alloc(nn);
+    if (st == cudaSuccess) st = lamd.alloc(n);
+  }
   if (st != cudaSuccess) return check_cuda(e, st, "scf allocation");
   int rc = one_body_device(e, S.p, T.p, V.p, s);
   if (rc) return rc;
@@ -329,10 +343,21 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   // a final FP64 build at the converged density: the energy is stationary in
   // D, so the density error the corrected builds leave enters it squared.
   // Convergence needs two corrected iterations after the last refresh.
-  const bool mixed = o->df && o->prec_mode == 1;
+  const bool incremental = o->df && o->prec_mode == 2;
+  const bool mixed = o->df && (o->prec_mode == 1 || incremental);
   const double mixed_switch = o->mixed_switch > 0.0 ? o->mixed_switch : 1e-3;
   const int refresh_every = o->mixed_refresh > 0 ? o->mixed_refresh : 0;
-  const bool corrected = mixed && refresh_every > 0;
+  const bool corrected = mixed && !incremental && refresh_every > 0;
+  // prec_mode 2: after the mixed phase an FP64 anchor build G64(D_ref), then
+  // F = H + G64(D_ref) + Gmixed(D - D_ref) with D - D_ref = 2 (C+ C+^T - C- C-^T)
+  // from its eigenvectors (rank <= 2 nocc), so the mixed error scales with
+  // ||D - D_ref||; a second anchor once ||dD|| < 100 densconverge
+  bool have_anchor = false;
+  int anchors = 0, since_anchor = 0;
+  double dd_now = 1e300;  // ||D - D_old||_F of the current iteration
+  std::vector<double> hlam(incremental ? n : 0), hscale(incremental ? n : 0);
+  DevBuf<double> dscale;
+  if (incremental && (st = dscale.alloc(n)) != cudaSuccess) return check_cuda(e, st, "scf scale");
   int fp64_after_switch = 0;
   bool switched = !mixed, have_delta = false;
   int build_kind = 0;  // of the last Fock build (trace)
@@ -471,6 +496,48 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     cudaEventDestroy(b);
     return rc2;
   };
+  // G = G64(D_ref) + Gmixed(D - D_ref) through two mixed DF builds of the
+  // scaled eigenvectors of D - D_ref (positive and negative parts)
+  auto incremental_fock = [&](double* G) -> int {
+    g.copy(D.p, t1.p, nn);
+    g.axpy(-1.0, Dref.p, t1.p, nn);
+    if (!syev(t1.p, Ud.p, lamd.p)) return set_error(e, JK_ERR_CUDA, "syevd(D - D_ref)");
+    cudaMemcpyAsync(hlam.data(), lamd.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    double lmax = 0.0;
+    for (int i = 0; i < n; ++i) lmax = std::max(lmax, std::fabs(hlam[i]));
+    const double thr = std::max(1e-10 * lmax, 1e-14);
+    int rm = 0, rp = 0;  // ascending eigenvalues: negative ones first, positive ones last
+    while (rm < n && rm < nocc && hlam[rm] < -thr) ++rm;
+    while (rp < n - rm && rp < nocc && hlam[n - 1 - rp] > thr) ++rp;
+    g.copy(Gref.p, G, nn);
+    for (int part = 0; part < 2; ++part) {
+      const int r = part ? rp : rm, c0 = part ? n - rp : 0;
+      if (r == 0) continue;
+      for (int j = 0; j < r; ++j) hscale[j] = std::sqrt(0.5 * std::fabs(hlam[c0 + j]));
+      cudaMemcpyAsync(dscale.p, hscale.data(), sizeof(double) * r, cudaMemcpyHostToDevice, s);
+      launch_scale_columns(Ud.p + (size_t)c0 * n, n, r, dscale.p, Cpm.p, s);
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, s);
+      int rc2 = df_jk_device(e, Cpm.p, r, 1, J.p, K.p, s);
+      cudaEventRecord(b, s);
+      cudaEventSynchronize(b);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      jk_ms += ms;
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      ++builds;
+      ++mixed_builds;
+      if (rc2) return rc2;
+      const double sg = part ? 1.0 : -1.0;  // G(D+) - G(D-)
+      g.axpy(2.0 * sg, J.p, G, nn);
+      g.axpy(-sg, K.p, G, nn);
+    }
+    return JK_OK;
+  };
   auto make_fock = [&]() -> int {
     if (!o->df) {
       g.copy(Finc.p, F.p, nn);
@@ -499,6 +566,21 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
       if (!switched) {
         build_kind = 1;
         rc2 = jk(nullptr, t2.p, 1);
+      } else if (incremental && (!have_anchor || (anchors < 2 && dd_now < 100.0 * o->densconverge))) {
+        build_kind = 0;  // FP64 anchor
+        if ((rc2 = jk(nullptr, Gref.p, 0))) return rc2;
+        g.copy(D.p, Dref.p, nn);
+        g.copy(Gref.p, t2.p, nn);
+        have_anchor = true;
+        ++anchors;
+        since_anchor = 0;
+        focks.clear();  // Fock matrices built around the old reference
+        diis.reset();
+        fock_iter = 0;
+      } else if (incremental) {
+        build_kind = 4;
+        if ((rc2 = incremental_fock(t2.p))) return rc2;
+        ++since_anchor;
       } else if (corrected && (!have_delta || since_refresh >= refresh_every)) {
         build_kind = 3;
         if ((rc2 = jk(nullptr, Delta.p, 1))) return rc2;
@@ -583,6 +665,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     g.copy(D.p, t1.p, nn);
     g.axpy(-1.0, Dold.p, t1.p, nn);
     dd = g.nrm2(t1.p, nn);
+    dd_now = dd;
     if (!switched) {  // takes effect in this iteration's build
       const double best = std::min(dd_hist[0], std::min(dd_hist[1], dd_hist[2]));
       if (dd < mixed_switch || (it >= 6 && dd > 0.5 * best)) switched = true;
@@ -599,7 +682,9 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     if (it > 2) average(weights);
     transform(F.p);
     // a mixed run converges only on FP64 (or FP64-corrected) builds
-    const bool precise = !mixed || (corrected ? (have_delta && since_refresh >= 2) : fp64_after_switch >= 2);
+    const bool precise = !mixed || (incremental ? (anchors >= 2 && since_anchor >= 2)
+                                                : corrected ? (have_delta && since_refresh >= 2)
+                                                            : fp64_after_switch >= 2);
     converged = dd < o->densconverge && delta < o->enconverge && precise;
     if (o->out_trace && it < o->maxiter) {
       double* tr = o->out_trace + (size_t)5 * it;

@@ -48,6 +48,7 @@ SIGNATURES = {
     "jk_df_setup": (_I, [_P]),
     "jk_df_set_range": (_I, [_P, _I, _I]),
     "jk_df_set_storage": (_I, [_P, _I]),
+    "jk_df_mp2": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "jk_df_storage": (_I, [_P]),
     "jk_df_set_tiled_blocks": (_I, [_P, _I, _I]),
     "jk_df": (_I, [_P, _P, _I, _I, _P, _P]),
@@ -227,6 +228,15 @@ class IntegralEngine:
 
     def df_setup(self):
         self._check(self.lib.jk_df_setup(self.h))
+
+    def df_mp2(self, C, eps, nocc, nfrozen=0):
+        """MP2::dfmp2 (src/mp2.cpp:477-583): DF-MP2 correlation energy for canonical
+        orbitals C (n x nmo) and energies eps; the nfrozen lowest occupied are frozen."""
+        C = np.asfortranarray(C, dtype=np.float64)
+        eps = np.ascontiguousarray(eps, dtype=np.float64)
+        e = ctypes.c_double(0.0)
+        self._check(self.lib.jk_df_mp2(self.h, _p(C), _p(eps), C.shape[1], nocc, nfrozen, ctypes.byref(e)))
+        return e.value
 
     DF_STORAGE = {"auto": 0, "unpacked": 1, "tiled": 2}
 

@@ -262,3 +262,27 @@ def eri3_deriv_block(obs, aux, sa, s2, s3, center, xyz):
     out = np.zeros(int(np.prod(n)))
     lib().orc_eri3_deriv_block(_bp(obs), _bp(aux), sa, s2, s3, center, xyz, _p(out))
     return out.reshape(n)
+
+
+def df_mp2(obs, aux, C, eps, nocc, nfrozen=0):
+    """MP2::dfmp2 (src/mp2.cpp:477-583): the explicit inverse metric (P|Q)^-1
+    (:498), the two-step MO transform of the packed (P|mn) (:526-552), and the
+    energy sum over i, a, j, b with (ia|jb) = B_ia (P|Q)^-1 B_jb (:554-581),
+    vectorised over a, b."""
+    n = obs.nbf
+    Tp = eri3(obs, aux)                       # (n(n+1)/2) x naux, row x(x+1)/2 + y
+    Vinv = np.linalg.inv(eri2(aux))
+    x, y = np.tril_indices(n)
+    T = np.zeros((n, n, Tp.shape[1]))
+    T[x, y] = Tp[x * (x + 1) // 2 + y]
+    T[y, x] = Tp[x * (x + 1) // 2 + y]
+    Co, Cv = C[:, nfrozen:nocc], C[:, nocc:]
+    B = np.einsum("mi,mnP,na->iaP", Co, T, Cv, optimize=True)
+    BV = B @ Vinv
+    eo, ev = eps[nfrozen:nocc], eps[nocc:C.shape[1]]
+    E = 0.0
+    for i in range(Co.shape[1]):
+        for j in range(Co.shape[1]):
+            v = B[i] @ BV[j].T                    # (ia|jb) over (a, b)
+            E += np.sum(v * (2.0 * v - v.T) / (eo[i] + eo[j] - ev[:, None] - ev[None, :]))
+    return E
