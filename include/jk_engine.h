@@ -232,8 +232,10 @@ typedef struct jk_scf_options {
                               builds to convergence after that (or, with mixed_refresh,
                               corrected mixed builds); 2 = the same mixed phase, then an FP64
                               anchor build G64(D_ref) and mixed builds of the low-rank change
-                              D - D_ref only (error proportional to ||D - D_ref||), with a second
-                              anchor once ||D - D_old||_F < 100 densconverge */
+                              D - D_ref only (error proportional to ||D - D_ref||); a new anchor
+                              when ||D - D_old||_F stalls, or falls below densconverge while
+                              ||D - D_ref||_F >= 100 densconverge (at most 8); converged only
+                              with ||D - D_ref||_F < 100 densconverge */
   double mixed_switch;     /* default 1e-3; the switch also happens when ||dD|| stalls */
   int mixed_refresh;       /* 0 (default): FP64 builds after the switch.  k > 0: mixed builds
                               plus the correction G64 - Gmixed refreshed every k iterations,

@@ -3,17 +3,19 @@
 // Same contraction as the FP64 path (compute_2body_fock_df, molecular2
 // src/fockbuild.cpp:621-659), with B = Bhi + Blo and C = Chi + Clo split into
 // BF16 pairs and every product formed as hi*hi + hi*lo + lo*hi with FP32
-// accumulation in tensor memory (~16 significant bits per operand):
+// accumulation in tensor memory (~16 significant bits per operand), restarted
+// every ACC_GROUP k-blocks and summed in registers:
 //   GEMM1  X[m][i] = sum_y B[m][y] C[y][i],  m = (x,K): persistent kernel over
 //          128-row tiles, TMA -> 4-stage smem ring -> tcgen05.mma (M=128,
 //          N=nocc padded to 16) -> double-buffered TMEM accumulators.  The
 //          epilogue re-splits X into BF16 hi/lo for GEMM2 and accumulates
 //          gamma_K = sum_{x,i} X[x][K][i] C[x][i] (FP64 atomics).
 //   GEMM2  K = X X^T over the naux*nocc index: 128x128 tiles of the lower
-//          triangle, split-K across the SMs, FP32 atomics.
+//          triangle, split-K across the SMs, FP64 register totals, FP64
+//          atomics.
 //   J      J[x][y] = sum_K gamma_K B[x][K][y] over y <= x: HBM-bound stream of
 //          the lower half of B (hi + lo).
-// One warp issues TMA, one issues MMA, four drain TMEM; all waits are bounded
+// One warp issues TMA, one issues MMA, the rest drain TMEM; all waits are bounded
 // and report through an error word instead of hanging.
 #include <algorithm>
 #include <cmath>
@@ -48,6 +50,7 @@ struct G1Params {
   __nv_bfloat16* Xhi;  // [m][NP]
   __nv_bfloat16* Xlo;
   double* gamma;
+  double* Kt;       // K accumulator: receives the diagonal lo*lo term
   int* err;
 };
 
@@ -61,21 +64,47 @@ struct G1Layout {
   static constexpr int TMEM_COLS = 2 * ACC_STRIDE;
 };
 
+// Accumulation groups.  tcgen05.mma accumulates in FP32 and its additions
+// lose low-order bits in one direction, so a long accumulation drifts toward
+// zero (about -1e-4 relative after ~2000 k-blocks).  The MMA warp therefore
+// restarts the TMEM accumulator every G1_GROUP (GEMM1) or ACC_GROUP (GEMM2)
+// k-blocks of 64 inner-index values and the epilogue adds the group partials
+// in registers with round-to-nearest arithmetic; the drift is then that of
+// one group.
+constexpr int G1_GROUP = 4;
+constexpr int ACC_GROUP = 4;
+
 // One epilogue warp's share of a GEMM1 tile: TMEM columns [16*C0, 16*C1) of
-// its 32 rows.  Releases the accumulator buffer as soon as the values are in
-// registers, then adds this share to gamma and writes X as BF16 hi/lo.
+// its 32 rows, summed over the tile's `ngroups` accumulation groups (global
+// group counter gt, buffer gt & 1).  Each buffer is released as soon as its
+// values are in registers; the sum is then added to gamma and written as
+// BF16 hi/lo.  Returns false when a wait timed out.
 template <int NP, int C0, int C1>
-__device__ __forceinline__ void g1_epilogue_part(uint32_t taddr, int m, const G1Params& P, uint64_t* tempty_b,
-                                                 int lane) {
+__device__ __forceinline__ bool g1_epilogue_tile(uint32_t tbase, int& gt, int ngroups, int m, const G1Params& P,
+                                                 uint64_t* tfull, uint64_t* tempty, int lane) {
+  using Lay = G1Layout<NP>;
   constexpr int NV = (C1 - C0) * 16;
   float v[NV > 0 ? NV : 1];
 #pragma unroll
-  for (int c = C0; c < C1; ++c) tmem_ld16(taddr + c * 16, v + (c - C0) * 16);
-  if constexpr (NV > 0) tmem_ld_wait();
-  tc_fence_before();
-  __syncwarp();
-  if (lane == 0) mbar_arrive(tempty_b);
-  if (NV == 0 || m >= P.M) return;
+  for (int i = 0; i < NV; ++i) v[i] = 0.0f;
+  for (int g = 0; g < ngroups; ++g, ++gt) {
+    const int b = gt & 1;
+    if (!mbar_wait(&tfull[b], (gt >> 1) & 1)) return false;
+    tc_fence_after();
+    const uint32_t taddr = tbase + b * Lay::ACC_STRIDE;
+#pragma unroll
+    for (int c = C0; c < C1; ++c) {
+      float w[16];
+      tmem_ld16(taddr + c * 16, w);
+      tmem_ld_wait();
+#pragma unroll
+      for (int e = 0; e < 16; ++e) v[(c - C0) * 16 + e] += w[e];
+    }
+    tc_fence_before();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&tempty[b]);
+  }
+  if (NV == 0 || m >= P.M) return true;
   const int x = m / P.naux, K = m - x * P.naux;
   const double* Cx = P.C + x;
   double g4[4] = {0.0, 0.0, 0.0, 0.0};
@@ -85,6 +114,7 @@ __device__ __forceinline__ void g1_epilogue_part(uint32_t taddr, int m, const G1
   atomicAdd(P.gamma + K, (g4[0] + g4[1]) + (g4[2] + g4[3]));
   uint4* oh = reinterpret_cast<uint4*>(P.Xhi + (size_t)m * NP + C0 * 16);
   uint4* ol = reinterpret_cast<uint4*>(P.Xlo + (size_t)m * NP + C0 * 16);
+  float lsq = 0.0f;
 #pragma unroll
   for (int c = 0; c < NV / 8; ++c) {
     __align__(16) __nv_bfloat16 h[8], l[8];
@@ -93,10 +123,24 @@ __device__ __forceinline__ void g1_epilogue_part(uint32_t taddr, int m, const G1
       const float f = v[c * 8 + e];
       h[e] = __float2bfloat16_rn(f);
       l[e] = __float2bfloat16_rn(f - __bfloat162float(h[e]));
+      const float lf = __bfloat162float(l[e]);
+      lsq = fmaf(lf, lf, lsq);
     }
     oh[c] = *reinterpret_cast<const uint4*>(h);
     ol[c] = *reinterpret_cast<const uint4*>(l);
   }
+  // GEMM2 forms hi*hi + hi*lo + lo*hi; the dropped lo*lo term averages out off
+  // the diagonal but is sum_k lo_k^2 > 0 on it, so it is added here (one
+  // atomic per warp when the warp's rows share x, as all but boundary rows do)
+  double lq = (double)lsq;
+  const unsigned mask = __activemask();
+  if (mask == 0xffffffffu && __all_sync(mask, x == __shfl_sync(mask, x, 0))) {
+    for (int o = 16; o > 0; o >>= 1) lq += __shfl_xor_sync(mask, lq, o);
+    if (lane == 0) atomicAdd(P.Kt + (size_t)x * P.n + x, lq);
+  } else {
+    atomicAdd(P.Kt + (size_t)x * P.n + x, lq);
+  }
+  return true;
 }
 
 constexpr int G1_EPI = 3;                            // epilogue warps per TMEM lane quadrant
@@ -168,41 +212,43 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
       constexpr uint32_t idesc = idesc_bf16_f32(BM, NP);
-      int it = 0, lt = 0;
+      int it = 0, gt = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < P.ntiles && ok; t += gridDim.x, ++lt) {
-        const int b = lt & 1;
-        const uint32_t u = lt >> 1;
-        if (!mbar_wait(&tempty[b], (u & 1) ^ 1)) {
-          report(P.err, ERR_WAIT_MMA);
-          break;
-        }
-        tc_fence_after();
-        const uint32_t d = tmem + b * Lay::ACC_STRIDE;
-        for (int kb = 0; kb < P.kblocks; ++kb, ++it) {
-          const int s = it % S;
-          const uint32_t j = it / S;
-          if (!mbar_wait(&full[s], j & 1)) {
+      for (int t = blockIdx.x; t < P.ntiles && ok; t += gridDim.x)
+        for (int kg = 0; kg < P.kblocks && ok; kg += G1_GROUP, ++gt) {
+          const int b = gt & 1;
+          if (!mbar_wait(&tempty[b], ((gt >> 1) & 1) ^ 1)) {
             report(P.err, ERR_WAIT_MMA);
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint8_t* st = smem + s * Lay::STAGE;
+          const uint32_t d = tmem + b * Lay::ACC_STRIDE;
+          const int kend = min(kg + G1_GROUP, P.kblocks);
+          for (int kb = kg; kb < kend; ++kb, ++it) {
+            const int s = it % S;
+            const uint32_t j = it / S;
+            if (!mbar_wait(&full[s], j & 1)) {
+              report(P.err, ERR_WAIT_MMA);
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint8_t* st = smem + s * Lay::STAGE;
 #pragma unroll
-          for (int k = 0; k < BK / 16; ++k) {
-            const uint64_t ah = sdesc_kmajor_sw128(st + k * 32);
-            const uint64_t al = sdesc_kmajor_sw128(st + TILE_A_BYTES + k * 32);
-            const uint64_t bh = sdesc_kmajor_sw128(st + 2 * TILE_A_BYTES + k * 32);
-            const uint64_t bl = sdesc_kmajor_sw128(st + 2 * TILE_A_BYTES + Lay::B_BYTES + k * 32);
-            umma_bf16(d, ah, bh, idesc, (kb > 0 || k > 0) ? 1u : 0u);
-            umma_bf16(d, ah, bl, idesc, 1u);
-            umma_bf16(d, al, bh, idesc, 1u);
+            for (int k = 0; k < BK / 16; ++k) {
+              const uint64_t ah = sdesc_kmajor_sw128(st + k * 32);
+              const uint64_t al = sdesc_kmajor_sw128(st + TILE_A_BYTES + k * 32);
+              const uint64_t bh = sdesc_kmajor_sw128(st + 2 * TILE_A_BYTES + k * 32);
+              const uint64_t bl = sdesc_kmajor_sw128(st + 2 * TILE_A_BYTES + Lay::B_BYTES + k * 32);
+              umma_bf16(d, ah, bh, idesc, (kb > kg || k > 0) ? 1u : 0u);
+              umma_bf16(d, ah, bl, idesc, 1u);
+              umma_bf16(d, al, bh, idesc, 1u);
+            }
+            umma_commit(&empty[s]);
           }
-          umma_commit(&empty[s]);
+          if (ok) umma_commit(&tfull[b]);
         }
-        if (ok) umma_commit(&tfull[b]);
-      }
       umma_commit(drain);  // every issued MMA has finished before TMEM is freed
       mbar_wait(drain, 0);
     }
@@ -210,24 +256,23 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
     const int q = warp & 3, part = (warp - 2) >> 2;
     constexpr int NCH = NP / 16;
     constexpr int CH1 = (NCH + G1_EPI - 1) / G1_EPI, CH2 = (2 * NCH + G1_EPI - 1) / G1_EPI;
-    int lt = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++lt) {
-      const int b = lt & 1;
-      const uint32_t u = lt >> 1;
-      if (!mbar_wait(&tfull[b], u & 1)) {
+    const int ngroups = (P.kblocks + G1_GROUP - 1) / G1_GROUP;
+    const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16);
+    int gt = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+      const int m = t * BM + 32 * q + lane;
+      static_assert(G1_EPI == 3, "chunk split below is written for three parts");
+      bool ok;
+      if (part == 0)
+        ok = g1_epilogue_tile<NP, 0, CH1>(tbase, gt, ngroups, m, P, tfull, tempty, lane);
+      else if (part == 1)
+        ok = g1_epilogue_tile<NP, CH1, CH2>(tbase, gt, ngroups, m, P, tfull, tempty, lane);
+      else
+        ok = g1_epilogue_tile<NP, CH2, NCH>(tbase, gt, ngroups, m, P, tfull, tempty, lane);
+      if (!ok) {
         report(P.err, ERR_WAIT_EPILOGUE);
         break;
       }
-      tc_fence_after();
-      const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16) + b * Lay::ACC_STRIDE;
-      const int m = t * BM + 32 * q + lane;
-      static_assert(G1_EPI == 3, "chunk split below is written for three parts");
-      if (part == 0)
-        g1_epilogue_part<NP, 0, CH1>(taddr, m, P, &tempty[b], lane);
-      else if (part == 1)
-        g1_epilogue_part<NP, CH1, CH2>(taddr, m, P, &tempty[b], lane);
-      else
-        g1_epilogue_part<NP, CH2, NCH>(taddr, m, P, &tempty[b], lane);
     }
   }
   tc_fence_before();
@@ -254,14 +299,22 @@ constexpr int G2_STAGE = 4 * TILE_A_BYTES;
 constexpr int G2_STAGES = 3;
 constexpr int G2_SMEM = G2_STAGES * G2_STAGE + 1024 + 1024;
 
-__global__ void __launch_bounds__(192, 1)
+constexpr int G2_EPI = 2;                            // epilogue warps per TMEM lane quadrant
+constexpr int G2_THREADS = 64 + 4 * 32 * G2_EPI;     // TMA warp, MMA warp, epilogue warps
+constexpr int G2_COLS = BM / G2_EPI;                 // accumulator columns per epilogue warp
+
+// Accumulation groups of ACC_GROUP k-blocks go to alternating TMEM buffers;
+// the epilogue adds each group's FP32 partial to FP64 totals in registers and
+// adds the totals to Kt once at the end.
+__global__ void __launch_bounds__(G2_THREADS, 1)
     k_gemm2(const __grid_constant__ CUtensorMap tXh, const __grid_constant__ CUtensorMap tXl, const G2Params P) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* full = (uint64_t*)(smem + G2_STAGES * G2_STAGE);
   uint64_t* empty = full + G2_STAGES;
   uint64_t* tfull = empty + G2_STAGES;
-  uint64_t* drain = tfull + 1;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* drain = tempty + 2;
   uint32_t* tmem_slot = (uint32_t*)(drain + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // which lower-triangle tile and which slice of the inner index
@@ -283,13 +336,16 @@ __global__ void __launch_bounds__(192, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(&tfull[0], 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4 * G2_EPI);
+    }
     mbar_init(drain, 1);
     fence_barrier_init();
     prefetch_tmap(&tXh);
     prefetch_tmap(&tXl);
   }
-  if (warp == 0) tmem_alloc(tmem_slot, 128);
+  if (warp == 0) tmem_alloc(tmem_slot, 2 * BM);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -322,52 +378,76 @@ __global__ void __launch_bounds__(192, 1)
     if (lane == 0 && have_work) {
       constexpr uint32_t idesc = idesc_bf16_f32(BM, BM);
       bool ok = true;
-      for (int kb = kb0, it = 0; kb < kb1; ++kb, ++it) {
-        const int s = it % G2_STAGES;
-        const uint32_t j = it / G2_STAGES;
-        if (!mbar_wait(&full[s], j & 1)) {
+      int it = 0, gt = 0;
+      for (int kg = kb0; kg < kb1 && ok; kg += ACC_GROUP, ++gt) {
+        const int b = gt & 1;
+        if (!mbar_wait(&tempty[b], ((gt >> 1) & 1) ^ 1)) {
           report(P.err, ERR_WAIT_MMA);
-          ok = false;
           break;
         }
         tc_fence_after();
-        const uint8_t* st = smem + s * G2_STAGE;
+        const uint32_t d = tmem + b * BM;
+        const int kend = min(kg + ACC_GROUP, kb1);
+        for (int kb = kg; kb < kend; ++kb, ++it) {
+          const int s = it % G2_STAGES;
+          const uint32_t j = it / G2_STAGES;
+          if (!mbar_wait(&full[s], j & 1)) {
+            report(P.err, ERR_WAIT_MMA);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint8_t* st = smem + s * G2_STAGE;
 #pragma unroll
-        for (int k = 0; k < BK / 16; ++k) {
-          const uint64_t ah = sdesc_kmajor_sw128(st + k * 32);
-          const uint64_t al = sdesc_kmajor_sw128(st + TILE_A_BYTES + k * 32);
-          const uint64_t bh = sdesc_kmajor_sw128(st + 2 * TILE_A_BYTES + k * 32);
-          const uint64_t bl = sdesc_kmajor_sw128(st + 3 * TILE_A_BYTES + k * 32);
-          umma_bf16(tmem, ah, bh, idesc, (it > 0 || k > 0) ? 1u : 0u);
-          umma_bf16(tmem, ah, bl, idesc, 1u);
-          umma_bf16(tmem, al, bh, idesc, 1u);
+          for (int k = 0; k < BK / 16; ++k) {
+            const uint64_t ah = sdesc_kmajor_sw128(st + k * 32);
+            const uint64_t al = sdesc_kmajor_sw128(st + TILE_A_BYTES + k * 32);
+            const uint64_t bh = sdesc_kmajor_sw128(st + 2 * TILE_A_BYTES + k * 32);
+            const uint64_t bl = sdesc_kmajor_sw128(st + 3 * TILE_A_BYTES + k * 32);
+            umma_bf16(d, ah, bh, idesc, (kb > kg || k > 0) ? 1u : 0u);
+            umma_bf16(d, ah, bl, idesc, 1u);
+            umma_bf16(d, al, bh, idesc, 1u);
+          }
+          umma_commit(&empty[s]);
         }
-        umma_commit(&empty[s]);
+        if (ok) umma_commit(&tfull[b]);
       }
-      if (ok) umma_commit(&tfull[0]);
       umma_commit(drain);
       mbar_wait(drain, 0);
     }
-  } else if (have_work) {
-    const int q = warp & 3;
-    if (!mbar_wait(&tfull[0], 0)) {
-      report(P.err, ERR_WAIT_EPILOGUE);
-    } else {
-      tc_fence_after();
-      const int x = tx * BM + 32 * q + lane;
-      const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16);
-#pragma unroll 1
-      for (int c = 0; c < BM / 16; ++c) {
-        float v[16];
-        tmem_ld16(taddr + c * 16, v);
-        tmem_ld_wait();
-        if (x < P.n) {
+  } else if (have_work) {  // warp w: TMEM lanes 32*(w%4).., columns [G2_COLS*part, +G2_COLS)
+    const int q = warp & 3, part = (warp - 2) >> 2;
+    const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + part * G2_COLS;
+    double acc[G2_COLS];
 #pragma unroll
-          for (int e = 0; e < 16; ++e) {
-            const int y = ty * BM + c * 16 + e;
-            if (y < P.n) atomicAdd(P.Kt + (size_t)y * P.n + x, (double)v[e]);
-          }
-        }
+    for (int e = 0; e < G2_COLS; ++e) acc[e] = 0.0;
+    bool ok = true;
+    for (int kg = kb0, gt = 0; kg < kb1; kg += ACC_GROUP, ++gt) {
+      const int b = gt & 1;
+      if (!mbar_wait(&tfull[b], (gt >> 1) & 1)) {
+        report(P.err, ERR_WAIT_EPILOGUE);
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+#pragma unroll
+      for (int c = 0; c < G2_COLS / 16; ++c) {
+        float v[16];
+        tmem_ld16(tbase + b * BM + c * 16, v);
+        tmem_ld_wait();
+#pragma unroll
+        for (int e = 0; e < 16; ++e) acc[c * 16 + e] += (double)v[e];
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[b]);
+    }
+    const int x = tx * BM + 32 * q + lane;
+    if (ok && x < P.n) {
+#pragma unroll
+      for (int e = 0; e < G2_COLS; ++e) {
+        const int y = ty * BM + part * G2_COLS + e;
+        if (y < P.n) atomicAdd(P.Kt + (size_t)y * P.n + x, acc[e]);
       }
     }
   }
@@ -375,7 +455,7 @@ __global__ void __launch_bounds__(192, 1)
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    tmem_dealloc(tmem, 128);
+    tmem_dealloc(tmem, 2 * BM);
   }
 }
 
@@ -591,6 +671,7 @@ int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double
   P1.Xhi = m.Xh.p;
   P1.Xlo = m.Xl.p;
   P1.gamma = d.gamma.p;
+  P1.Kt = m.Kt.p;
   P1.err = m.err.p;
   cudaError_t st = dispatch_g1(NP, m.maps, P1, std::min(nsm, P1.ntiles), s);
   if (st != cudaSuccess) return check_cuda(e, st, "gemm1 launch");
@@ -605,7 +686,7 @@ int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double
   P2.err = m.err.p;
   st = cudaFuncSetAttribute(k_gemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, G2_SMEM);
   if (st != cudaSuccess) return check_cuda(e, st, "gemm2 attribute");
-  k_gemm2<<<P2.ntiles_u * P2.splits, 192, G2_SMEM, s>>>(m.maps[4], m.maps[5], P2);
+  k_gemm2<<<P2.ntiles_u * P2.splits, G2_THREADS, G2_SMEM, s>>>(m.maps[4], m.maps[5], P2);
   st = cudaGetLastError();
   if (st != cudaSuccess) return check_cuda(e, st, "gemm2 launch");
   stage_mark(e, 2, s);
@@ -667,7 +748,7 @@ cudaError_t launch_gemm2(const CUtensorMap& tXh, const CUtensorMap& tXl, int n, 
   P2.err = err;
   cudaError_t st = cudaFuncSetAttribute(k_gemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, G2_SMEM);
   if (st != cudaSuccess) return st;
-  k_gemm2<<<P2.ntiles_u * P2.splits, 192, G2_SMEM, s>>>(tXh, tXl, P2);
+  k_gemm2<<<P2.ntiles_u * P2.splits, G2_THREADS, G2_SMEM, s>>>(tXh, tXl, P2);
   return cudaGetLastError();
 }
 

@@ -85,6 +85,7 @@ struct S1Params {
   __nv_bfloat16* Xh;  // [x][K_local][NPX]
   __nv_bfloat16* Xl;
   double* gamma;     // global fitted index
+  double* Kt;        // K accumulator: receives the diagonal lo*lo term
   int* err;
 };
 
@@ -95,18 +96,40 @@ __device__ __forceinline__ void s1_item(const S1Params& P, int item, int& Kl, in
   Kl = r / P.nt;
 }
 
-// One epilogue warp's share: TMEM columns [16*C0, 16*C1) of its 32 rows.
+// Accumulation groups of S1_GROUP 64-wide k chunks: the MMA warp restarts the
+// TMEM accumulator for each group and the epilogue sums the FP32 group
+// partials with round-to-nearest additions, so the downward drift of the
+// tensor-core accumulation stays that of one group.
+constexpr int S1_GROUP = 4;
+
+// One epilogue warp's share of a work item: TMEM columns [16*C0, 16*C1) of its
+// 32 rows summed over the item's accumulation groups (global group counter gt,
+// buffer gt & 1, each released as soon as it is in registers), then added to
+// gamma and written as BF16 hi/lo.  Returns false when a wait timed out.
 template <int C0, int C1>
-__device__ __forceinline__ void s1_epilogue_part(uint32_t taddr, int x, int Kl, int h, const S1Params& P,
-                                                 uint64_t* tempty_b, int lane) {
+__device__ __forceinline__ bool s1_epilogue_item(uint32_t tbase, int& gt, int ngroups, int x, int Kl, int h,
+                                                 const S1Params& P, uint64_t* tfull, uint64_t* tempty, int lane) {
   constexpr int NV = (C1 - C0) * 16;
   float v[NV];
 #pragma unroll
-  for (int c = C0; c < C1; ++c) tmem_ld16(taddr + c * 16, v + (c - C0) * 16);
-  tmem_ld_wait();
-  tc_fence_before();
-  __syncwarp();
-  if (lane == 0) mbar_arrive(tempty_b);
+  for (int i = 0; i < NV; ++i) v[i] = 0.0f;
+  for (int g = 0; g < ngroups; ++g, ++gt) {
+    const int b = gt & 1;
+    if (!mbar_wait(&tfull[b], (gt >> 1) & 1)) return false;
+    tc_fence_after();
+    const uint32_t taddr = tbase + b * S1_ACC;
+#pragma unroll
+    for (int c = C0; c < C1; ++c) {
+      float w[16];
+      tmem_ld16(taddr + c * 16, w);
+      tmem_ld_wait();
+#pragma unroll
+      for (int e = 0; e < 16; ++e) v[(c - C0) * 16 + e] += w[e];
+    }
+    tc_fence_before();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&tempty[b]);
+  }
   const int i0 = h * SN + C0 * 16;
   if (x < P.n) {
     double g4[4] = {0.0, 0.0, 0.0, 0.0};
@@ -118,6 +141,7 @@ __device__ __forceinline__ void s1_epilogue_part(uint32_t taddr, int x, int Kl, 
   const size_t row = ((size_t)x * P.wstride + Kl) * P.NPX + i0;
   uint4* oh = reinterpret_cast<uint4*>(P.Xh + row);
   uint4* ol = reinterpret_cast<uint4*>(P.Xl + row);
+  float lsq = 0.0f;
 #pragma unroll
   for (int c = 0; c < NV / 8; ++c) {
     __align__(16) __nv_bfloat16 hh[8], ll[8];
@@ -126,10 +150,15 @@ __device__ __forceinline__ void s1_epilogue_part(uint32_t taddr, int x, int Kl, 
       const float f = v[c * 8 + e];
       hh[e] = __float2bfloat16_rn(f);
       ll[e] = __float2bfloat16_rn(f - __bfloat162float(hh[e]));
+      const float lf = __bfloat162float(ll[e]);
+      lsq = fmaf(lf, lf, lsq);
     }
     oh[c] = *reinterpret_cast<const uint4*>(hh);
     ol[c] = *reinterpret_cast<const uint4*>(ll);
   }
+  // the lo*lo term GEMM2 drops is sum_k lo_k^2 > 0 on the diagonal of K
+  if (x < P.n) atomicAdd(P.Kt + (size_t)x * P.n + x, (double)lsq);
+  return true;
 }
 
 __global__ void __launch_bounds__(S1_THREADS, 1)
@@ -216,76 +245,78 @@ __global__ void __launch_bounds__(S1_THREADS, 1)
     if (lane == 0) {  // MMA issuer
       constexpr uint32_t idk = idesc_bf16_f32(TB, SN);
       constexpr uint32_t idm = idesc_bf16_f32_amn(TB, SN);
-      int it = 0, lt = 0;
+      int it = 0, gt = 0;
       bool ok = true;
-      for (int item = blockIdx.x; item < P.nitems && ok; item += gridDim.x, ++lt) {
+      for (int item = blockIdx.x; item < P.nitems && ok; item += gridDim.x) {
         int Kl, I, h;
         s1_item(P, item, Kl, I, h);
-        const int b = lt & 1;
-        const uint32_t u = lt >> 1;
-        if (!mbar_wait(&tempty[b], (u & 1) ^ 1)) {
-          report(P.err, ERR_WAIT_MMA);
-          break;
-        }
-        tc_fence_after();
-        const uint32_t d = tmem + b * S1_ACC;
-        for (int q = 0; q < kchunks; ++q, ++it) {
-          const int J = q >> 1;
-          const int s = it % S;
-          const uint32_t j = it / S;
-          if (!mbar_wait(&full[s], j & 1)) {
+        for (int qg = 0; qg < kchunks && ok; qg += S1_GROUP, ++gt) {
+          const int b = gt & 1;
+          if (!mbar_wait(&tempty[b], ((gt >> 1) & 1) ^ 1)) {
             report(P.err, ERR_WAIT_MMA);
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint8_t* st = smem + s * S1_STAGE;
-          const bool mn = J > I;
-#pragma unroll
-          for (int k = 0; k < SBK / 16; ++k) {
-            uint64_t ah, al;
-            if (!mn) {
-              ah = sdesc_kmajor_sw128(st + k * 32);
-              al = sdesc_kmajor_sw128(st + S1_A + k * 32);
-            } else {
-              ah = sdesc_mnmajor_sw128(st + k * 2048, S1_A / 2, 1024);
-              al = sdesc_mnmajor_sw128(st + S1_A + k * 2048, S1_A / 2, 1024);
+          const uint32_t d = tmem + b * S1_ACC;
+          const int qend = min(qg + S1_GROUP, kchunks);
+          for (int q = qg; q < qend; ++q, ++it) {
+            const int J = q >> 1;
+            const int s = it % S;
+            const uint32_t j = it / S;
+            if (!mbar_wait(&full[s], j & 1)) {
+              report(P.err, ERR_WAIT_MMA);
+              ok = false;
+              break;
             }
-            const uint64_t bh = sdesc_kmajor_sw128(st + 2 * S1_A + k * 32);
-            const uint64_t bl = sdesc_kmajor_sw128(st + 2 * S1_A + S1_C + k * 32);
-            const uint32_t id = mn ? idm : idk;
-            umma_bf16(d, ah, bh, id, (q > 0 || k > 0) ? 1u : 0u);
-            umma_bf16(d, ah, bl, id, 1u);
-            umma_bf16(d, al, bh, id, 1u);
+            tc_fence_after();
+            const uint8_t* st = smem + s * S1_STAGE;
+            const bool mn = J > I;
+#pragma unroll
+            for (int k = 0; k < SBK / 16; ++k) {
+              uint64_t ah, al;
+              if (!mn) {
+                ah = sdesc_kmajor_sw128(st + k * 32);
+                al = sdesc_kmajor_sw128(st + S1_A + k * 32);
+              } else {
+                ah = sdesc_mnmajor_sw128(st + k * 2048, S1_A / 2, 1024);
+                al = sdesc_mnmajor_sw128(st + S1_A + k * 2048, S1_A / 2, 1024);
+              }
+              const uint64_t bh = sdesc_kmajor_sw128(st + 2 * S1_A + k * 32);
+              const uint64_t bl = sdesc_kmajor_sw128(st + 2 * S1_A + S1_C + k * 32);
+              const uint32_t id = mn ? idm : idk;
+              umma_bf16(d, ah, bh, id, (q > qg || k > 0) ? 1u : 0u);
+              umma_bf16(d, ah, bl, id, 1u);
+              umma_bf16(d, al, bh, id, 1u);
+            }
+            umma_commit(&empty[s]);
           }
-          umma_commit(&empty[s]);
+          if (ok) umma_commit(&tfull[b]);
         }
-        if (ok) umma_commit(&tfull[b]);
       }
       umma_commit(drain);  // every issued MMA has finished before TMEM is freed
       mbar_wait(drain, 0);
     }
   } else {  // epilogue: warp w drains TMEM lanes 32*(w%4).. and part (w-2)/4 of the 10 column chunks
     const int qd = warp & 3, part = (warp - 2) >> 2;
-    int lt = 0;
-    for (int item = blockIdx.x; item < P.nitems; item += gridDim.x, ++lt) {
+    const int ngroups = (kchunks + S1_GROUP - 1) / S1_GROUP;
+    const uint32_t tbase = tmem + ((uint32_t)(32 * qd) << 16);
+    int gt = 0;
+    for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
       int Kl, I, h;
       s1_item(P, item, Kl, I, h);
-      const int b = lt & 1;
-      const uint32_t u = lt >> 1;
-      if (!mbar_wait(&tfull[b], u & 1)) {
+      const int x = TB * I + 32 * qd + lane;
+      bool ok;
+      if (part == 0)
+        ok = s1_epilogue_item<0, 4>(tbase, gt, ngroups, x, Kl, h, P, tfull, tempty, lane);
+      else if (part == 1)
+        ok = s1_epilogue_item<4, 7>(tbase, gt, ngroups, x, Kl, h, P, tfull, tempty, lane);
+      else
+        ok = s1_epilogue_item<7, 10>(tbase, gt, ngroups, x, Kl, h, P, tfull, tempty, lane);
+      if (!ok) {
         report(P.err, ERR_WAIT_EPILOGUE);
         break;
       }
-      tc_fence_after();
-      const uint32_t taddr = tmem + ((uint32_t)(32 * qd) << 16) + b * S1_ACC;
-      const int x = TB * I + 32 * qd + lane;
-      if (part == 0)
-        s1_epilogue_part<0, 4>(taddr, x, Kl, h, P, &tempty[b], lane);
-      else if (part == 1)
-        s1_epilogue_part<4, 7>(taddr, x, Kl, h, P, &tempty[b], lane);
-      else
-        s1_epilogue_part<7, 10>(taddr, x, Kl, h, P, &tempty[b], lane);
     }
   }
   tc_fence_before();
@@ -670,6 +701,7 @@ static int tiled_mixed(jk_engine* e, const double* dC, int nocc, double* dJ, dou
     P.Xh = T.Xh.p;
     P.Xl = T.Xl.p;
     P.gamma = d.gamma.p;
+    P.Kt = T.Kt.p;
     P.err = T.err.p;
     k_gemm1_sym<<<std::min(nsm, P.nitems), S1_THREADS, S1_SMEM, s>>>(T.maps[0], T.maps[1], T.maps[2], T.maps[3],
                                                                        T.maps[4], T.maps[5], P);
@@ -791,12 +823,19 @@ static int tiled_fp64(jk_engine* e, const double* dC, int nocc, double* dJ, doub
   if (st == cudaSuccess) st = cv.alloc(naux);
   if (st == cudaSuccess) st = tv.alloc(naux);
   if (st != cudaSuccess) return check_cuda(e, st, "tiled FP64 scratch");
+  // the mixed build's X block is released (its next call allocates it again)
+  // so that the occupied slices, each one more integral pass, are as wide as
+  // the memory allows
+  if (T.Xh.p) {
+    T.Xh.reset();
+    T.Xl.reset();
+  }
   // occupied slice: X' (npad x naux x oc) and a Y batch of XB rows must fit
   constexpr int XB = 64;
   size_t fr = 0, tt = 0;
   cudaMemGetInfo(&fr, &tt);
   const double per_o = 8.0 * (double)(npad + XB) * naux;
-  int oc = (int)std::min<double>(nocc, std::floor(0.85 * (double)fr / per_o));
+  int oc = (int)std::min<double>(nocc, std::floor(0.94 * (double)fr / per_o));
   if (T.oc_max > 0) oc = std::min(oc, T.oc_max);
   if (oc < 1) return set_error(e, JK_ERR_NOMEM, "tiled FP64 DF: no room for one occupied orbital's X'");
   const int nch = (nocc + oc - 1) / oc;

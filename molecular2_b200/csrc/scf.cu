@@ -351,10 +351,16 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
   // prec_mode 2: after the mixed phase an FP64 anchor build G64(D_ref), then
   // F = H + G64(D_ref) + Gmixed(D - D_ref) with D - D_ref = 2 (C+ C+^T - C- C-^T)
   // from its eigenvectors (rank <= 2 nocc), so the mixed error scales with
-  // ||D - D_ref||; a second anchor once ||dD|| < 100 densconverge
-  bool have_anchor = false;
+  // ||D - D_ref||.  A new anchor is taken at the current density when the
+  // density change stalls where the noise of Gmixed(D - D_ref) dominates (no
+  // 15% gain on the best ||dD|| since the anchor after four incremental
+  // builds, with ||dD|| below 2% of ||D - D_ref||),
+  // or when ||dD|| < densconverge while ||D - D_ref|| >= 100 densconverge;
+  // a run converges only with ||D - D_ref|| < 100 densconverge.
+  bool have_anchor = false, want_anchor = false;
   int anchors = 0, since_anchor = 0;
-  double dd_now = 1e300;  // ||D - D_old||_F of the current iteration
+  double ref_norm = 0.0, dd_best = 1e300;
+  constexpr int MAX_ANCHORS = 8;
   std::vector<double> hlam(incremental ? n : 0), hscale(incremental ? n : 0);
   DevBuf<double> dscale;
   if (incremental && (st = dscale.alloc(n)) != cudaSuccess) return check_cuda(e, st, "scf scale");
@@ -566,7 +572,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
       if (!switched) {
         build_kind = 1;
         rc2 = jk(nullptr, t2.p, 1);
-      } else if (incremental && (!have_anchor || (anchors < 2 && dd_now < 100.0 * o->densconverge))) {
+      } else if (incremental && (!have_anchor || want_anchor)) {
         build_kind = 0;  // FP64 anchor
         if ((rc2 = jk(nullptr, Gref.p, 0))) return rc2;
         g.copy(D.p, Dref.p, nn);
@@ -574,6 +580,7 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
         have_anchor = true;
         ++anchors;
         since_anchor = 0;
+        dd_best = 1e300;
         focks.clear();  // Fock matrices built around the old reference
         diis.reset();
         fock_iter = 0;
@@ -665,7 +672,15 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     g.copy(D.p, t1.p, nn);
     g.axpy(-1.0, Dold.p, t1.p, nn);
     dd = g.nrm2(t1.p, nn);
-    dd_now = dd;
+    if (incremental && have_anchor) {
+      g.copy(D.p, t1.p, nn);
+      g.axpy(-1.0, Dref.p, t1.p, nn);
+      ref_norm = g.nrm2(t1.p, nn);
+      const bool stall = since_anchor >= 4 && dd > 0.85 * dd_best && dd < 0.02 * ref_norm;
+      const bool settle = dd < o->densconverge && ref_norm >= 100.0 * o->densconverge;
+      want_anchor = (stall || settle) && anchors < MAX_ANCHORS;
+      dd_best = std::min(dd_best, dd);
+    }
     if (!switched) {  // takes effect in this iteration's build
       const double best = std::min(dd_hist[0], std::min(dd_hist[1], dd_hist[2]));
       if (dd < mixed_switch || (it >= 6 && dd > 0.5 * best)) switched = true;
@@ -682,7 +697,8 @@ int scf_rhf(jk_engine* e, const jk_scf_options* o, jk_scf_result* r) {
     if (it > 2) average(weights);
     transform(F.p);
     // a mixed run converges only on FP64 (or FP64-corrected) builds
-    const bool precise = !mixed || (incremental ? (anchors >= 2 && since_anchor >= 2)
+    if (incremental && build_kind == 0) ref_norm = 0.0;  // this iteration's build was the anchor at D
+    const bool precise = !mixed || (incremental ? (have_anchor && ref_norm < 100.0 * o->densconverge)
                                                 : corrected ? (have_delta && since_refresh >= 2)
                                                             : fp64_after_switch >= 2);
     converged = dd < o->densconverge && delta < o->enconverge && precise;

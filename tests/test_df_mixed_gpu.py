@@ -59,3 +59,46 @@ def test_mixed_scf_energy_within_1e6():
     assert r64.converged and rmx.converged
     assert rmx.mixed_builds > 0
     assert abs(rmx.energy - r64.energy) < 1e-6
+
+
+@pytest.mark.parametrize("storage", ["unpacked", "tiled"])
+def test_mixed_k_diagonal_unbiased(storage):
+    """The tensor-core FP32 accumulation drifts toward zero over long sums and
+    GEMM2's dropped lo*lo term is positive on the diagonal; with accumulation
+    groups and the diagonal lo*lo term added, the mean signed relative error
+    of diag(K) stays at the rounding level (it was -3e-5 at this size before)."""
+    mol = geometry.water_cluster(16, 9.0, seed=16)
+    obs, aux = BasisSet(mol, "cc-pvdz"), BasisSet(mol, "vdz-jkfit")
+    eng = _engine(obs, aux)
+    eng.set_df_storage(storage)
+    eng.df_setup()
+    r, ex = eng.scf_rhf(mol.nocc, mol.enuc(), df=True, densconverge=1e-6, enconverge=1e-9, want=True,
+                        guess="soad")
+    C = np.ascontiguousarray(ex["C"][:, :mol.nocc])
+    _, K64 = eng.jk_df(C, 0)
+    _, K = eng.jk_df(C, 1)
+    bias = float(np.mean((np.diag(K) - np.diag(K64)) / np.diag(K64)))
+    ek = np.max(np.abs(K - K64)) / np.max(np.abs(K64))
+    print(f"{storage}: mean signed rel err of diag K {bias:.2e}, max rel err {ek:.2e}")
+    assert abs(bias) < 3e-6
+    assert ek < 3e-5
+
+
+def test_incremental_scf_energy_within_1e6():
+    """prec_mode 2: FP64 anchors plus split-BF16 builds of D - D_ref."""
+    mol = geometry.water_cluster(8, 7.0, seed=8)
+    obs, aux = BasisSet(mol, "aug-cc-pvdz"), BasisSet(mol, "avdz-jkfit")
+    eng = _engine(obs, aux)
+    eng.set_df_storage("tiled")
+    eng.df_setup()
+    Fs = eng.soad_fock(1e-12)
+    kw = dict(df=True, densconverge=1e-5, enconverge=1e-8, maxiter=60, guess_fock=Fs)
+    r64, _ = eng.scf_rhf(mol.nocc, mol.enuc(), **kw)
+    r2, ex = eng.scf_rhf(mol.nocc, mol.enuc(), prec_mode=2, **kw)
+    kinds = ex["trace"][:, 3].astype(int)
+    print(f"FP64 {r64.energy:.10f} ({r64.iterations} it), incremental {r2.energy:.10f} ({r2.iterations} it, "
+          f"{r2.jk_builds - r2.mixed_builds} anchors, kinds {kinds.tolist()})")
+    assert r64.converged and r2.converged
+    assert 1 <= r2.jk_builds - r2.mixed_builds < r64.jk_builds
+    assert 4 in kinds
+    assert abs(r2.energy - r64.energy) < 1e-6
