@@ -35,6 +35,7 @@ itself needs libint2/Eigen and cannot be built here; its packed FP64 B for
 this system would be 264 GB), on a bounded sample of the fitting functions,
 extrapolated linearly in naux.
 --profile runs only the set-up and the timed builds (for ncu launch lists);
+--profile-direct water8|c20h42 runs only two direct J/K builds;
 --precision fp64 times FP64 builds instead of mixed ones; --workload water16aug
 is the small case of the tiled kernels used for ncu captures.
 With --gpus N > 1 every rank runs its own replica of the workload (the
@@ -554,6 +555,27 @@ def run_ours(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def profile_direct(local, name):
+    """Driver for ncu launch lists of the direct J/K kernels: engine, SOAD
+    Fock, one diagonalisation, two jk_direct builds of (H2O)8/cc-pVDZ
+    ("water8") or C20H42/6-311G** ("c20h42")."""
+    import scipy.linalg as sl
+    from molecular2_b200 import geometry
+    from molecular2_b200.basis import BasisSet
+    from molecular2_b200.engine import IntegralEngine
+    mol, basis = (geometry.water8(), "cc-pvdz") if name == "water8" else (geometry.c20h42(), "6-311g**")
+    eng = IntegralEngine(BasisSet(mol, basis), device=local)
+    S, _, _ = eng.one_body()
+    _, C = sl.eigh(eng.soad_fock(), S)
+    D = 2.0 * C[:, :mol.nocc] @ C[:, :mol.nocc].T
+    for _ in range(2):
+        t = time.perf_counter()
+        eng.jk_direct(D, 1e-12)
+        print(json.dumps({"profile_direct": name, "ms": 1e3 * (time.perf_counter() - t),
+                          "quartets": eng.last_quartets()}), flush=True)
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -567,12 +589,17 @@ def main():
     ap.add_argument("--clock-dir", default=None, help="where the nvidia-smi clock samples go (default: a temp dir)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the smaller workloads")
+    ap.add_argument("--profile-direct", default=None, choices=["water8", "c20h42"],
+                    help="only run two direct J/K builds (driver for ncu launch lists)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.profile_direct:
+        profile_direct(local, args.profile_direct)
         return
     if world > 1:
         import datetime

@@ -168,6 +168,13 @@ int jk_df_uhf_device(jk_engine* e, const double* dCa, int na, const double* dCb,
  * which inverts (P|Q) explicitly where this uses its Cholesky factor. */
 int jk_df_mp2(jk_engine* e, const double* C, const double* eps, int nmo, int nocc, int nfrozen, double* emp2);
 
+/* Failure-detection check of the bounded mbarrier wait every tensor-core
+ * kernel uses: one launch waits `polls` times on a barrier that nothing
+ * completes (*timed_out = 1 when the wait gave up and the kernel returned)
+ * and on one that has completed (*completed_timed_out = 0).  No molecular2
+ * counterpart; the engine's device must be current. */
+int jk_wait_selftest(jk_engine* e, unsigned polls, int* timed_out, int* completed_timed_out);
+
 /* Layout of the fitted tensor, chosen before jk_df_setup (molecular2 keeps one
  * packed FP64 (n(n+1)/2) x naux matrix, src/fockbuild.cpp:598-619, which
  * stops fitting in device memory near n = 2600, naux = 9600):

@@ -700,6 +700,20 @@ int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double
   return check_cuda(e, cudaGetLastError(), "mixed DF launch");
 }
 
+// The bounded wait of the tensor-core kernels on a barrier that nothing
+// completes (status[0]: 1 if it gave up) and on one that completes (status[1]:
+// 1 if it gave up), with `limit` polls.
+__global__ void k_wait_selftest(uint32_t limit, int* status) {
+  __shared__ __align__(8) uint64_t bar[2];
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar[0], 1);
+  mbar_init(&bar[1], 1);
+  fence_barrier_init();
+  mbar_arrive(&bar[1]);
+  status[0] = mbar_wait_n(&bar[0], 0, limit) ? 0 : 1;
+  status[1] = mbar_wait_n(&bar[1], 0, limit) ? 0 : 1;
+}
+
 int df_mixed_error(jk_engine* e) {
   if (e->tiled.ready) return df_tiled_error(e);
   if (!e->mixed.err.p) return JK_OK;
@@ -759,3 +773,25 @@ cudaError_t launch_finalize_mixed(int n, const double* Kt, double* J, double* K,
 }
 
 }  // namespace m2
+
+using namespace m2;
+
+extern "C" int jk_wait_selftest(jk_engine* e, unsigned polls, int* timed_out, int* completed_timed_out) {
+  if (!e || !timed_out || !completed_timed_out || polls == 0) return JK_ERR_ARG;
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess || cur != e->device)
+    return set_error(e, JK_ERR_ARG, "jk_wait_selftest: the engine's device must be current");
+  DevBuf<int> st;
+  cudaError_t r = st.alloc(2);
+  if (r == cudaSuccess) r = cudaMemsetAsync(st.p, 0xff, 2 * sizeof(int), e->stream);
+  if (r != cudaSuccess) return check_cuda(e, r, "jk_wait_selftest");
+  k_wait_selftest<<<1, 32, 0, e->stream>>>(polls, st.p);
+  int h[2] = {-1, -1};
+  r = cudaGetLastError();
+  if (r == cudaSuccess) r = cudaMemcpyAsync(h, st.p, sizeof(h), cudaMemcpyDeviceToHost, e->stream);
+  if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
+  if (r != cudaSuccess) return check_cuda(e, r, "jk_wait_selftest");
+  *timed_out = h[0];
+  *completed_timed_out = h[1];
+  return JK_OK;
+}

@@ -99,8 +99,10 @@ __device__ __forceinline__ void s1_item(const S1Params& P, int item, int& Kl, in
 // Accumulation groups of S1_GROUP 64-wide k chunks: the MMA warp restarts the
 // TMEM accumulator for each group and the epilogue sums the FP32 group
 // partials with round-to-nearest additions, so the downward drift of the
-// tensor-core accumulation stays that of one group.
-constexpr int S1_GROUP = 4;
+// tensor-core accumulation stays that of one group.  With two accumulator
+// buffers the MMA warp runs at most two groups ahead of the epilogue, so a
+// group must outlast the epilogue's per-item work (gamma, split, stores).
+constexpr int S1_GROUP = 8;
 
 // One epilogue warp's share of a work item: TMEM columns [16*C0, 16*C1) of its
 // 32 rows summed over the item's accumulation groups (global group counter gt,

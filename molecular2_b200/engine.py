@@ -49,6 +49,7 @@ SIGNATURES = {
     "jk_df_set_range": (_I, [_P, _I, _I]),
     "jk_df_set_storage": (_I, [_P, _I]),
     "jk_df_mp2": (_I, [_P, _P, _P, _I, _I, _I, _P]),
+    "jk_wait_selftest": (_I, [_P, ctypes.c_uint, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "jk_df_storage": (_I, [_P]),
     "jk_df_set_tiled_blocks": (_I, [_P, _I, _I]),
     "jk_df": (_I, [_P, _P, _I, _I, _P, _P]),
@@ -237,6 +238,13 @@ class IntegralEngine:
         e = ctypes.c_double(0.0)
         self._check(self.lib.jk_df_mp2(self.h, _p(C), _p(eps), C.shape[1], nocc, nfrozen, ctypes.byref(e)))
         return e.value
+
+    def wait_selftest(self, polls=1024):
+        """Bounded-wait check: (gave up on a barrier nothing completes,
+        gave up on a completed barrier) -- (True, False) when the waits work."""
+        a, b = _I(-1), _I(-1)
+        self._check(self.lib.jk_wait_selftest(self.h, polls, ctypes.byref(a), ctypes.byref(b)))
+        return bool(a.value), bool(b.value)
 
     DF_STORAGE = {"auto": 0, "unpacked": 1, "tiled": 2}
 
