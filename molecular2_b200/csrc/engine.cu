@@ -349,6 +349,11 @@ int jk_create(const jk_basis* obs, const jk_basis* aux, int natom, const double*
   e->device = device;
   cudaError_t st = cudaSetDevice(device);
   if (st == cudaSuccess) st = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  for (int i = 0; i < jk_engine::NCLS_STREAMS && st == cudaSuccess; ++i) {
+    st = cudaStreamCreateWithFlags(&e->cls_stream[i], cudaStreamNonBlocking);
+    if (st == cudaSuccess) st = cudaEventCreateWithFlags(&e->cls_join[i], cudaEventDisableTiming);
+  }
+  if (st == cudaSuccess) st = cudaEventCreateWithFlags(&e->cls_fork, cudaEventDisableTiming);
   if (st != cudaSuccess) {
     rc = check_cuda(e, st, "jk_create: device/stream");
     *out = e;
@@ -381,12 +386,38 @@ void jk_destroy(jk_engine* e) {
   for (auto& ev : e->ev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : e->kev) cudaEventDestroy(ev);
+  for (int i = 0; i < jk_engine::NCLS_STREAMS; ++i) {
+    if (e->cls_stream[i]) cudaStreamSynchronize(e->cls_stream[i]);
+    if (e->cls_stream[i]) cudaStreamDestroy(e->cls_stream[i]);
+    if (e->cls_join[i]) cudaEventDestroy(e->cls_join[i]);
+  }
+  if (e->cls_fork) cudaEventDestroy(e->cls_fork);
   cudaStream_t s = e->stream;
   delete e;  // frees device buffers
   if (s) cudaStreamDestroy(s);
 }
 
 const char* jk_last_error(const jk_engine* e) { return e ? e->err.c_str() : "null engine"; }
+
+namespace m2 {
+ClassStreams::ClassStreams(jk_engine* e_, cudaStream_t s_) : e(e_), s(s_) {
+  cudaEventRecord(e->cls_fork, s);
+  for (int i = 0; i < jk_engine::NCLS_STREAMS; ++i) cudaStreamWaitEvent(e->cls_stream[i], e->cls_fork, 0);
+}
+cudaStream_t ClassStreams::next(double cost) {
+  int best = 0;
+  for (int i = 1; i < jk_engine::NCLS_STREAMS; ++i)
+    if (load[i] < load[best]) best = i;
+  load[best] += cost;
+  return e->cls_stream[best];
+}
+void ClassStreams::join() {
+  for (int i = 0; i < jk_engine::NCLS_STREAMS; ++i) {
+    cudaEventRecord(e->cls_join[i], e->cls_stream[i]);
+    cudaStreamWaitEvent(s, e->cls_join[i], 0);
+  }
+}
+}  // namespace m2
 
 int jk_sizes(const jk_engine* e, int* n, int* naux, int* nshell) {
   if (!e) return JK_ERR_ARG;

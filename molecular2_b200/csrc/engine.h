@@ -132,6 +132,11 @@ struct TiledDF {
 struct jk_engine {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // side streams of the per-class kernel launches (direct J/K, gradient):
+  // forked from and joined back to the call's stream with events
+  static constexpr int NCLS_STREAMS = 8;
+  cudaStream_t cls_stream[NCLS_STREAMS] = {};
+  cudaEvent_t cls_fork = nullptr, cls_join[NCLS_STREAMS] = {};
   cublasHandle_t cublas = nullptr;
   cusolverDnHandle_t cusolver = nullptr;
   std::string err;
@@ -221,6 +226,19 @@ void launch_final_to_cart(const jk_engine* e, const double* Dfinal, double* Dcar
 void launch_cart_to_final_sym(const jk_engine* e, const double* Xcart, double scale, double* Xfinal, cudaStream_t s);
 void launch_shell_norms(const jk_engine* e, const double* Dfinal, double* Dnorm, double* Dmax, cudaStream_t s);
 void launch_add(const double* a, const double* b, double* c, size_t n, cudaStream_t s);  // c = a + b
+
+// Per-class launches on side streams: ClassStreams cs(e, s) makes every side
+// stream wait for the work already queued on s; cs.next(cost) picks the side
+// stream with the least estimated cost queued so far (longest-first order
+// packs best); cs.join() makes s wait for all of them.
+struct ClassStreams {
+  jk_engine* e;
+  cudaStream_t s;
+  double load[jk_engine::NCLS_STREAMS] = {};
+  ClassStreams(jk_engine* e_, cudaStream_t s_);
+  cudaStream_t next(double cost);
+  void join();
+};
 int direct_jk_uhf_device(jk_engine* e, const double* dDa, const double* dDb, double precision, double mult,
                          double* dJa, double* dJb, double* dKa, double* dKb, cudaStream_t s);
 }  // namespace m2

@@ -7,6 +7,7 @@
 // term runs over the same unique shell quartets as the reference: both shell
 // pairs in the overlap-screened pair list (|S block| >= 1e-12 or same centre,
 // src/integrals.cpp:515-566) and max6(|D| blocks) Q_ab Q_cd >= precision.
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -139,16 +140,30 @@ int grad_rhf_device(jk_engine* e, const double* dD, const double* dW, double pre
   P.boys = e->boys.p;
   P.grad = g2e;
   P.kchunk = 64;  // one ket per thread (64-thread blocks)
+  // the class launches run on the engine's side streams, longest first (the
+  // gradient is accumulated with atomics, so they commute)
+  static const double ncp[6] = {1, 3, 9, 6, 18, 36};
+  struct Item {
+    int A, B;
+    double cost;
+  };
+  std::vector<Item> items;
   for (int A = 0; A < NPAIRCLASS && with_2e; ++A)
-    for (int B = 0; B <= A; ++B) {
-      if (!e->pcls[A].npair || !e->pcls[B].npair) continue;
-      P.bra = view(e->pcls[A]);
-      P.ket = view(e->pcls[B]);
-      P.bra_sig = sig[A].p;
-      P.ket_sig = sig[B].p;
-      P.same_class = (A == B);
-      launch_grad2e(A, B, P, e->pcls[A].npair, e->pcls[B].npair, s);
-    }
+    for (int B = 0; B <= A; ++B)
+      if (e->pcls[A].npair && e->pcls[B].npair)
+        items.push_back({A, B, (double)e->pcls[A].npair * e->pcls[B].npair * ncp[A] * ncp[B] * (A == B ? 0.5 : 1.0)});
+  std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.cost > b.cost; });
+  ClassStreams cs(e, s);
+  for (const Item& it : items) {
+    Grad2eParams Q = P;
+    Q.bra = view(e->pcls[it.A]);
+    Q.ket = view(e->pcls[it.B]);
+    Q.bra_sig = sig[it.A].p;
+    Q.ket_sig = sig[it.B].p;
+    Q.same_class = (it.A == it.B);
+    launch_grad2e(it.A, it.B, Q, e->pcls[it.A].npair, e->pcls[it.B].npair, cs.next(it.cost));
+  }
+  cs.join();
   for (int k = 0; k < NPAIRCLASS; ++k) {
     if (!e->pcls[k].npair) continue;
     Grad1eParams Q{};

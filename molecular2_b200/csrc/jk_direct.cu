@@ -5,8 +5,10 @@
 // six angular classes ss, ps, pp, ds, dp, dd and, inside a class, sorted by
 // their Schwarz bound Q_ab (descending).  A unique shell quartet is a pair of
 // pairs {ab, cd}: class(ab) > class(cd), or the same class with index(cd) <=
-// index(ab).  One kernel instantiation per class pair (21 for l <= 2); a block
-// owns one bra pair and a chunk of kets, one thread one quartet.  Because kets
+// index(ab).  One kernel instantiation per class pair (21 for l <= 2), the 21
+// launches of a build spread longest first over the engine's side streams so
+// that they run concurrently; a block owns one bra pair and a chunk of kets,
+// one thread one quartet.  Because kets
 // are Q-sorted, the kets that can pass Q_ab Q_cd Dmax >= precision form a
 // prefix found by binary search; each quartet then applies molecular2's
 // screen max6(|D| shell blocks) Q_ab Q_cd >= precision (:111-115).
@@ -164,6 +166,35 @@ static int ket_chunk(int nbra, int nket_max) {
   return k;
 }
 
+// Rough relative cost of one class launch (Cartesian products of the pair
+// classes ss ps pp ds dp dd times the pair counts): orders the launches
+// longest first over the side streams.
+static double class_cost(int A, int B, int nbra, int nket) {
+  static const double ncp[6] = {1, 3, 9, 6, 18, 36};
+  return (double)nbra * nket * ncp[A] * ncp[B] * (A == B ? 0.5 : 1.0);
+}
+
+// Every (bra class, ket class) launch of one build, longest first, spread over
+// the engine's side streams so that the small d classes run beside the large
+// ones instead of one after another; J, K and the counters are accumulated
+// with atomics, so the launches commute.
+template <class Launch>
+static void launch_classes(jk_engine* e, cudaStream_t s, Launch&& launch) {
+  struct Item {
+    int A, B;
+    double cost;
+  };
+  std::vector<Item> items;
+  for (int A = 0; A < NPAIRCLASS; ++A)
+    for (int B = 0; B <= A; ++B)
+      if (e->pcls[A].npair && e->pcls[B].npair)
+        items.push_back({A, B, class_cost(A, B, e->pcls[A].npair, e->pcls[B].npair)});
+  std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.cost > b.cost; });
+  ClassStreams cs(e, s);
+  for (const Item& it : items) launch(it.A, it.B, cs.next(it.cost));
+  cs.join();
+}
+
 static void launch_jk(int A, int B, const JKParams& Pin, int nbra, int nket_max, cudaStream_t s, int nden = 1) {
   JKParams P = Pin;
   P.kchunk = ket_chunk(nbra, nket_max);
@@ -216,17 +247,14 @@ int direct_jk_device(jk_engine* e, const double* dD, double precision, double mu
   P.boys = e->boys.p;
   P.counter = counter;
   P.kchunk = 128;  // one ket per thread: small classes still spread over the SMs
-  for (int A = 0; A < NPAIRCLASS; ++A)
-    for (int B = 0; B <= A; ++B) {
-      const PairClassDev& bra = e->pcls[A];
-      const PairClassDev& ket = e->pcls[B];
-      if (bra.npair == 0 || ket.npair == 0) continue;
-      P.bra = view(bra);
-      P.ket = view(ket);
-      P.same_class = (A == B);
-      P.work = e->class_work.p + 3 * (A * NPAIRCLASS + B);
-      launch_jk(A, B, P, bra.npair, ket.npair, s);
-    }
+  launch_classes(e, s, [&](int A, int B, cudaStream_t cs) {
+    JKParams Q = P;
+    Q.bra = view(e->pcls[A]);
+    Q.ket = view(e->pcls[B]);
+    Q.same_class = (A == B);
+    Q.work = e->class_work.p + 3 * (A * NPAIRCLASS + B);
+    launch_jk(A, B, Q, e->pcls[A].npair, e->pcls[B].npair, cs);
+  });
   // J = 1/4 (J + J^T) mult, K = 1/2 * 1/4 (K + K^T) mult  (src/fockbuild.cpp:146-149, 161-162)
   launch_cart_to_final_sym(e, e->Jcart.p, 0.25 * mult, dJ, s);
   launch_cart_to_final_sym(e, e->Kcart.p, 0.125 * mult, dK, s);
@@ -276,17 +304,14 @@ int direct_jk_uhf_device(jk_engine* e, const double* dDa, const double* dDb, dou
     return check_cuda(e, st, "jk_direct_uhf work counters");
   cudaMemsetAsync(e->class_work.p, 0, sizeof(unsigned long long) * 3 * NPAIRCLASS * NPAIRCLASS, s);
   e->class_work_valid = true;
-  for (int A = 0; A < NPAIRCLASS; ++A)
-    for (int B = 0; B <= A; ++B) {
-      const PairClassDev& bra = e->pcls[A];
-      const PairClassDev& ket = e->pcls[B];
-      if (bra.npair == 0 || ket.npair == 0) continue;
-      P.bra = view(bra);
-      P.ket = view(ket);
-      P.same_class = (A == B);
-      P.work = e->class_work.p + 3 * (A * NPAIRCLASS + B);
-      launch_jk(A, B, P, bra.npair, ket.npair, s, 2);
-    }
+  launch_classes(e, s, [&](int A, int B, cudaStream_t cs) {
+    JKParams Q = P;
+    Q.bra = view(e->pcls[A]);
+    Q.ket = view(e->pcls[B]);
+    Q.same_class = (A == B);
+    Q.work = e->class_work.p + 3 * (A * NPAIRCLASS + B);
+    launch_jk(A, B, Q, e->pcls[A].npair, e->pcls[B].npair, cs, 2);
+  });
   launch_cart_to_final_sym(e, Jc2.p, 0.25 * mult, dJa, s);
   launch_cart_to_final_sym(e, Jc2.p + ncc, 0.25 * mult, dJb, s);
   launch_cart_to_final_sym(e, Kc2.p, 0.125 * mult, dKa, s);
@@ -379,16 +404,13 @@ int direct_jk_noalloc(jk_engine* e, const double* dD, double precision, double m
   P.counter = counter;
   P.dstride = NOALLOC_CC;
   P.kchunk = 128;  // one ket per thread: small classes still spread over the SMs
-  for (int A = 0; A < NPAIRCLASS; ++A)
-    for (int B = 0; B <= A; ++B) {
-      const PairClassDev& bra = e->pcls[A];
-      const PairClassDev& ket = e->pcls[B];
-      if (bra.npair == 0 || ket.npair == 0) continue;
-      P.bra = view(bra);
-      P.ket = view(ket);
-      P.same_class = (A == B);
-      launch_jk(A, B, P, bra.npair, ket.npair, s);
-    }
+  launch_classes(e, s, [&](int A, int B, cudaStream_t cs) {
+    JKParams Q = P;
+    Q.bra = view(e->pcls[A]);
+    Q.ket = view(e->pcls[B]);
+    Q.same_class = (A == B);
+    launch_jk(A, B, Q, e->pcls[A].npair, e->pcls[B].npair, cs);
+  });
   launch_cart_to_final_sym(e, Jc, 0.25 * mult, dJ, s);
   launch_cart_to_final_sym(e, Kc, 0.125 * mult, dK, s);
   return check_cuda(e, cudaGetLastError(), "jk_direct_noalloc launch");
