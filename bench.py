@@ -80,7 +80,7 @@ def workload(name):
     return _CACHE[name]
 
 
-def config(name, mol, obs, aux, world=1):
+def config(name, mol, obs, aux, world=1, stored_bytes=None):
     w = WORKLOADS[name]
     gb = obs.nbf * obs.nbf * aux.nbf
     return {"workload": f"{w['label']} DF-JK build (n={obs.nbf}, naux={aux.nbf}, nocc={mol.nocc}), "
@@ -89,7 +89,7 @@ def config(name, mol, obs, aux, world=1):
                          "corrections",
             "storage": w["storage"],
             "l2": "inputs larger than L2 (fitted tensor %.1f GB split BF16 per build)"
-                  % ((gb / 2 if w["storage"] == "tiled" else gb) * 4 / 1e9),
+                  % ((stored_bytes if stored_bytes else (gb / 2 if w["storage"] == "tiled" else gb) * 4) / 1e9),
             "parallelism": "single GPU" if world == 1 else f"{world} independent replicas, one per GPU"}
 
 
@@ -212,16 +212,16 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- roofline
-def roofline_tiled(n, naux, nocc, st):
+def roofline_tiled(n, naux, nocc, st, stored_bytes):
     """Tiled mixed build.  st = [GEMM1 total ms, GEMM2 total ms, J ms,
     finalize ms, blocks].  Algorithmic work (B counted unpacked): GEMM1
     X = B C is 2 n^2 o naux flops, GEMM2 K = X X^T n(n+1) o naux flops; J
-    reads the stored tiles (split BF16) once."""
+    reads the stored tiles (split BF16, stored_bytes) once."""
     hbm, bf16, src = peaks()
     nt = (n + 127) // 128
     g1_flops = 2.0 * n * n * nocc * naux
     g2_flops = 1.0 * n * (n + 1) * nocc * naux
-    j_bytes = naux * (nt * (nt + 1) // 2) * 128 * 128 * 4.0
+    j_bytes = float(stored_bytes)
     nhalf = (nocc + 159) // 160
     g1_exec = 3 * 2.0 * (nt * 128) ** 2 * (nhalf * 160) * naux      # split products over padded tiles
     g1, g2, jm, fm, blocks = st[:5]
@@ -483,7 +483,9 @@ def run_ours(args, rank, world, local):
     eng.set_profiling(False)
     st = list(acc / nprof)
     tiled = eng.df_storage == "tiled"
-    roofline = roofline_tiled(n, naux, nocc, st) if tiled else roofline_unpacked(n, naux, nocc, st)
+    stored = eng.df_tensor_bytes if tiled else None
+    roofline = (roofline_tiled(n, naux, nocc, st, stored) if tiled
+                else roofline_unpacked(n, naux, nocc, st))
     # mixed J/K error against an FP64 build at the same orbitals
     Jm, Km = dJ.clone(), dK.clone()
     t = time.perf_counter()
@@ -549,7 +551,7 @@ def run_ours(args, rank, world, local):
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3->f32",
                 "data": "synthetic (seeded geometry; basis data from molecular2's library)",
-                "config": config(name, mol, obs, aux, world), "e2e": e2e, "roofline": roofline,
+                "config": config(name, mol, obs, aux, world, stored), "e2e": e2e, "roofline": roofline,
                 "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches * args.steps, "scf": scf,
                 "jk_builds_per_s": jk_rates, "gradient": gradient, "df_setup_s": setup_s, "extras": extra}
         print(json.dumps(line), flush=True)

@@ -188,6 +188,11 @@ int jk_wait_selftest(jk_engine* e, unsigned polls, int* timed_out, int* complete
 int jk_df_set_storage(jk_engine* e, int mode);
 int jk_df_storage(const jk_engine* e);
 
+/* Device bytes of the fitted tensor as stored (tiled: the split-BF16 tiles;
+ * unpacked: FP64 B plus its split-BF16 copy once a mixed build made it); 0
+ * before jk_df_setup.  Measurement only; no molecular2 counterpart. */
+long long jk_df_tensor_bytes(const jk_engine* e);
+
 /* Tiled storage only: caps on the block of fitted functions a mixed build
  * contracts at once (its X block) and on the occupied slice of one FP64
  * integral pass (0 = size them from free device memory, the default).  Small

@@ -479,25 +479,43 @@ static int tile_integrals(jk_engine* e, int t, double* T, cudaStream_t s) {
   int I, J;
   tile_of(t, I, J);
   cudaMemsetAsync(T, 0, sizeof(double) * TB * (size_t)naux * TB, s);
+  // the (fitting l, pair class) launches write disjoint parts of T: they run
+  // longest first on the side streams (cost: pairs x fitting functions x
+  // Cartesian sizes), so that the small ones fill the tails of the large ones
+  static const double ncp[NPAIRCLASS] = {1, 3, 9, 6, 18, 36};
+  struct Item {
+    int l, pc;
+    double cost;
+  };
+  Item items[(MAX_L_AUX + 1) * NPAIRCLASS];
+  int nitems = 0;
   for (int l = 0; l <= MAX_L_AUX; ++l) {
     if (!e->aux_by_l_count[l]) continue;
     for (int pc = 0; pc < NPAIRCLASS; ++pc) {
       const long long o0 = D.list_off[(size_t)t * NPAIRCLASS + pc], o1 = D.list_off[(size_t)t * NPAIRCLASS + pc + 1];
-      if (o1 == o0) continue;
-      const Eri3Params P = eri3_params(e, l, pc);
-      Eri3TileArgs A{};
-      A.plist = D.plist.p + o0;
-      A.nlist = (int)(o1 - o0);
-      A.x0 = TB * I;
-      A.y0 = TB * J;
-      A.naux = naux;
-      A.T = T;
-      if (l == 0) launch_eri3_tile_l0(pc, P, A, s);
-      if (l == 1) launch_eri3_tile_l1(pc, P, A, s);
-      if (l == 2) launch_eri3_tile_l2(pc, P, A, s);
-      if (l == 3) launch_eri3_tile_l3(pc, P, A, s);
+      if (o1 > o0) items[nitems++] = {l, pc, (double)(o1 - o0) * e->aux_by_l_count[l] * ncp[pc] * (l + 1) * (l + 2)};
     }
   }
+  std::sort(items, items + nitems, [](const Item& a, const Item& b) { return a.cost > b.cost; });
+  ClassStreams cs(e, s);
+  for (int k = 0; k < nitems; ++k) {
+    const int l = items[k].l, pc = items[k].pc;
+    const long long o0 = D.list_off[(size_t)t * NPAIRCLASS + pc];
+    const Eri3Params P = eri3_params(e, l, pc);
+    Eri3TileArgs A{};
+    A.plist = D.plist.p + o0;
+    A.nlist = (int)(D.list_off[(size_t)t * NPAIRCLASS + pc + 1] - o0);
+    A.x0 = TB * I;
+    A.y0 = TB * J;
+    A.naux = naux;
+    A.T = T;
+    cudaStream_t q = cs.next(items[k].cost);
+    if (l == 0) launch_eri3_tile_l0(pc, P, A, q);
+    if (l == 1) launch_eri3_tile_l1(pc, P, A, q);
+    if (l == 2) launch_eri3_tile_l2(pc, P, A, q);
+    if (l == 3) launch_eri3_tile_l3(pc, P, A, q);
+  }
+  cs.join();
   return check_cuda(e, cudaGetLastError(), "tile integrals");
 }
 
@@ -1008,6 +1026,15 @@ extern "C" int jk_df_set_tiled_blocks(jk_engine* e, int waux_max, int oc_max) {
   e->tiled.NPX_cap = 0;  // re-plan the mixed scratch on the next build
   e->tiled.NPX = 0;
   return JK_OK;
+}
+
+extern "C" long long jk_df_tensor_bytes(const jk_engine* e) {
+  if (!e) return -1;
+  if (e->tiled.ready) return (long long)(e->tiled.Bh.n + e->tiled.Bl.n) * (long long)sizeof(__nv_bfloat16);
+  if (e->df.ready)
+    return (long long)e->df.B64.n * (long long)sizeof(double) +
+           (long long)(e->mixed.Bh.n + e->mixed.Bl.n) * (long long)sizeof(__nv_bfloat16);
+  return 0;
 }
 
 extern "C" int jk_df_storage(const jk_engine* e) {

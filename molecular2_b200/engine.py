@@ -51,6 +51,7 @@ SIGNATURES = {
     "jk_df_mp2": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "jk_wait_selftest": (_I, [_P, ctypes.c_uint, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "jk_df_storage": (_I, [_P]),
+    "jk_df_tensor_bytes": (ctypes.c_longlong, [_P]),
     "jk_df_set_tiled_blocks": (_I, [_P, _I, _I]),
     "jk_df": (_I, [_P, _P, _I, _I, _P, _P]),
     "jk_df_device": (_I, [_P, _P, _I, _I, _P, _P, _P]),
@@ -263,6 +264,11 @@ class IntegralEngine:
     @property
     def df_storage(self):
         return {0: None, 1: "unpacked", 2: "tiled"}[int(self.lib.jk_df_storage(self.h))]
+
+    @property
+    def df_tensor_bytes(self):
+        """Device bytes of the fitted tensor as stored (0 before df_setup)."""
+        return int(self.lib.jk_df_tensor_bytes(self.h))
 
     @property
     def df_range(self):

@@ -61,6 +61,7 @@ def lib():
             "orc_grad2e": (None, [P, P, i, P, P, d, P, P, i]),
             "orc_eri3_deriv_block": (None, [P, P, i, i, i, i, i, P]),
             "orc_eri4_deriv_block": (None, [P, i, i, i, i, i, i, P]),
+            "orc_df_grad_contract": (None, [P, P, P, P, i, P, P, P, i]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -262,6 +263,42 @@ def eri3_deriv_block(obs, aux, sa, s2, s3, center, xyz):
     out = np.zeros(int(np.prod(n)))
     lib().orc_eri3_deriv_block(_bp(obs), _bp(aux), sa, s2, s3, center, xyz, _p(out))
     return out.reshape(n)
+
+
+def df_grad2e(obs, aux, Cocc, nthreads=None):
+    """Two-electron part of the gradient of the density-fitted RHF energy
+    (the DF J/K of compute_2body_fock_df, src/fockbuild.cpp:585-660, with
+    D = 2 C C^T), natom x 3.  With T = (P|mn), V = (P|Q), d = T.D,
+    c = V^-1 d, W_P,ij = sum_Q V^-1_PQ (Q|ij) and
+    G_P,mn = sum_ij C_mi C_nj W_P,ij:
+      E_J = 1/2 d^T V^-1 d,  E_K = -sum_ij (ij|ij)_fit,
+      dE = sum (P|mn)' [c_P D_mn - 2 G_P,mn] + sum (P|Q)' [-1/2 c_P c_Q + sum_ij W_P,ij W_Q,ij],
+    the derivative integrals from the oracle's Obara-Saika/HGP derivative
+    blocks (orc_df_grad_contract)."""
+    n, naux = obs.nbf, aux.nbf
+    C = np.asarray(Cocc, dtype=np.float64)
+    Tp = eri3(obs, aux)                                   # packed (n(n+1)/2) x naux
+    T = np.zeros((naux, n, n))
+    iu = np.tril_indices(n)
+    T[:, iu[0], iu[1]] = Tp.T
+    T[:, iu[1], iu[0]] = Tp.T
+    V = eri2(aux)
+    D = 2.0 * C @ C.T
+    d = np.einsum("pmn,mn->p", T, D)
+    c = np.linalg.solve(V, d)
+    Tij = np.einsum("mi,pmn,nj->pij", C, T, C)
+    W = np.linalg.solve(V, Tij.reshape(naux, -1)).reshape(Tij.shape)
+    G = np.einsum("mi,pij,nj->pmn", C, W, C)
+    M3 = np.ascontiguousarray(c[:, None, None] * D[None, :, :] - 2.0 * G)
+    Wf = W.reshape(naux, -1)
+    M2 = np.ascontiguousarray(-0.5 * np.outer(c, c) + Wf @ Wf.T)
+    natom = obs.mol.natom
+    ob_atom = np.ascontiguousarray(obs.atom, dtype=np.int32)
+    ax_atom = np.ascontiguousarray(aux.atom, dtype=np.int32)
+    g = np.zeros(3 * natom)
+    lib().orc_df_grad_contract(_bp(obs), _bp(aux), _p(ob_atom), _p(ax_atom), natom, _p(M3), _p(M2), _p(g),
+                               nthreads or os.cpu_count() or 1)
+    return g.reshape(natom, 3)
 
 
 def df_mp2(obs, aux, C, eps, nocc, nfrozen=0):

@@ -1386,6 +1386,63 @@ void orc_eri3_deriv_block(const orc_basis* obs, const orc_basis* aux, int sa, in
   std::memcpy(out, v.data(), v.size() * sizeof(double));
 }
 
+// Two-electron part of the density-fitted RHF gradient, the contraction step
+// (test restatement of the derivative of the DF energy of
+// src/fockbuild.cpp:585-660): with the three-index weights M3[P][m][n]
+// (naux x n x n, n fastest) and the metric weights M2[P][Q] (naux x naux),
+//   grad[3 A + x] = sum_{P,m,n} d(P|mn)/dA_x M3[P][m][n]
+//                 + sum_{P,Q}   d(P|Q)/dA_x  M2[P][Q],
+// every derivative integral from shell_eri_deriv (all shell combinations, no
+// screening).  The weights come from oracle.df_grad2e.
+void orc_df_grad_contract(const orc_basis* obs, const orc_basis* aux, const int* obs_atom, const int* aux_atom,
+                          int natom, const double* M3, const double* M2, double* grad, int nthreads) {
+  Basis B = make_basis(obs), Ba = make_basis(aux);
+  const int ns = (int)B.sh.size(), na = (int)Ba.sh.size(), n = B.n, naux = Ba.n;
+  if (nthreads < 1) nthreads = 1;
+  std::vector<std::vector<double>> gt(nthreads, std::vector<double>(3 * (size_t)natom, 0.0));
+  parallel_for(na, nthreads, [&](int sa, int t) {
+    double* g = gt[t].data();
+    std::vector<double> buf;
+    const Shell u = unit_shell(Ba.sh[sa].A);
+    const int np = Ba.sh[sa].nbf();
+    for (int s2 = 0; s2 < ns; ++s2)
+      for (int s3 = 0; s3 < ns; ++s3) {
+        const Shell* sh[4] = {&Ba.sh[sa], &u, &B.sh[s2], &B.sh[s3]};
+        const int n2 = B.sh[s2].nbf(), n3 = B.sh[s3].nbf();
+        const int centre_atom[4] = {aux_atom[sa], -1, obs_atom[s2], obs_atom[s3]};
+        for (int c : {0, 2, 3})
+          for (int x = 0; x < 3; ++x) {
+            shell_eri_deriv(sh, c, x, buf);
+            double acc = 0.0;
+            for (int fp = 0, f = 0; fp < np; ++fp)
+              for (int f2 = 0; f2 < n2; ++f2)
+                for (int f3 = 0; f3 < n3; ++f3, ++f)
+                  acc += buf[f] * M3[((size_t)(Ba.off[sa] + fp) * n + B.off[s2] + f2) * n + B.off[s3] + f3];
+            g[3 * centre_atom[c] + x] += acc;
+          }
+      }
+    for (int sb = 0; sb < na; ++sb) {
+      const Shell u2 = unit_shell(Ba.sh[sb].A);
+      const Shell* sh[4] = {&Ba.sh[sa], &u, &Ba.sh[sb], &u2};
+      const int nq = Ba.sh[sb].nbf();
+      const int centre_atom[4] = {aux_atom[sa], -1, aux_atom[sb], -1};
+      for (int c : {0, 2})
+        for (int x = 0; x < 3; ++x) {
+          shell_eri_deriv(sh, c, x, buf);
+          double acc = 0.0;
+          for (int fp = 0, f = 0; fp < np; ++fp)
+            for (int fq = 0; fq < nq; ++fq, ++f) acc += buf[f] * M2[(size_t)(Ba.off[sa] + fp) * naux + Ba.off[sb] + fq];
+          g[3 * centre_atom[c] + x] += acc;
+        }
+    }
+  });
+  for (int k = 0; k < 3 * natom; ++k) {
+    double a = 0.0;
+    for (int t = 0; t < nthreads; ++t) a += gt[t][k];
+    grad[k] = a;
+  }
+}
+
 void orc_eri4_deriv_block(const orc_basis* obs, int s1, int s2, int s3, int s4, int center, int xyz, double* out) {
   Basis B = make_basis(obs);
   const Shell* sh[4] = {&B.sh[s1], &B.sh[s2], &B.sh[s3], &B.sh[s4]};

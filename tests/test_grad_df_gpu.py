@@ -5,7 +5,9 @@ invariance, and against the 4-index gradient (the two differ only by the
 fitting error).
 
 Bars: central differences (step 1e-4 bohr) within 1e-6 Eh/bohr; the sum over
-atoms within 1e-9; DF vs 4-index gradient within 1e-3 Eh/bohr.
+atoms within 1e-9; DF vs 4-index gradient within 1e-3 Eh/bohr; the
+two-electron part against the oracle's restatement (oracle.df_grad2e, analytic
+derivative integrals) within 1e-9 Eh/bohr.
 """
 import numpy as np
 import pytest
@@ -56,3 +58,24 @@ def test_df_gradient_close_to_4index():
     W = C @ np.diag(ex["eps"][:o]) @ C.T
     g_4, _ = eng.compute_forces(ex["D"], W)
     assert np.max(np.abs(g_df - g_4)) < 1e-3
+
+
+@pytest.mark.parametrize("k,obs,aux,storage", [(1, "cc-pvdz", "vdz-jkfit", "unpacked"),
+                                               (2, "cc-pvdz", "vdz-jkfit", "unpacked"),
+                                               (2, "cc-pvdz", "vdz-jkfit", "tiled"),
+                                               (1, "aug-cc-pvdz", "avdz-jkfit", "tiled")])
+def test_df_gradient_2e_matches_oracle(k, obs, aux, storage):
+    import oracle
+    from molecular2_b200.engine import IntegralEngine
+    mol = geometry.water() if k == 1 else geometry.water_cluster(k, 5.0, seed=3)
+    b, a = BasisSet(mol, obs), BasisSet(mol, aux)
+    eng = IntegralEngine(b, a)
+    eng.set_df_storage(storage)
+    r, ex = eng.scf_rhf(mol.nocc, mol.enuc(), want=True, **CONV)
+    assert r.converged
+    o = mol.nocc
+    _, g2 = eng.compute_forces_df(ex["C"][:, :o], ex["eps"][:o])
+    g2_ref = oracle.df_grad2e(b, a, ex["C"][:, :o])
+    err = np.max(np.abs(g2 - g2_ref))
+    print(f"(H2O){k} {obs} {storage}: DF two-electron gradient vs oracle {err:.2e}")
+    assert err < 1e-9
