@@ -253,7 +253,7 @@ def roofline_unpacked(n, naux, nocc, st):
     g1_bytes = 2 * n * naux * ldb * 2 + 2 * n * naux * NP * 2
     ach = g1_bytes / st[0] / 1e6
     return {"kernel": "k_gemm1", "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-            "traffic": None, "peak_source": src, "algorithmic_bytes_per_launch": g1_bytes,
+            "traffic": traffic("k_gemm1"), "peak_source": src, "algorithmic_bytes_per_launch": g1_bytes,
             "stages_ms": {"gemm1": st[0], "gemm2": st[1], "J": st[2], "finalize": st[3]}}
 
 
