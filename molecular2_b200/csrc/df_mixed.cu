@@ -10,9 +10,8 @@
 //          N=nocc padded to 16) -> double-buffered TMEM accumulators.  The
 //          epilogue re-splits X into BF16 hi/lo for GEMM2 and accumulates
 //          gamma_K = sum_{x,i} X[x][K][i] C[x][i] (FP64 atomics).
-//   GEMM2  K = X X^T over the naux*nocc index: 128x128 tiles of the lower
-//          triangle, split-K across the SMs, FP64 register totals, FP64
-//          atomics.
+//   GEMM2  K = X X^T over the naux*nocc index: 128x256 blocks of the lower
+//          triangle, split-K across the SMs, register totals, FP64 atomics.
 //   J      J[x][y] = sum_K gamma_K B[x][K][y] over y <= x: HBM-bound stream of
 //          the lower half of B (hi + lo).
 // One warp issues TMA, one issues MMA, the rest drain TMEM; all waits are bounded
@@ -284,28 +283,49 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
 }
 
 // ---------------------------------------------------------------- GEMM2
+// K = X X^T over blocks of 128 rows x 256 columns of the lower triangle (row
+// tile tx, column tiles 2cp and 2cp+1 <= tx + 1): each k block loads 128 rows
+// of A and 256 rows of B, 4/3 the flops per loaded byte of square 128 x 128
+// tiles.  Blocks whose second column tile lies above the diagonal (or past the
+// last row) run N = 128.
 struct G2Params {
   int n;
   int kblocks;      // (naux*NP)/64
   int ntile_n;      // ceil(n/128)
-  int ntiles_u;     // lower-triangle tiles
+  int nblocks;      // lower-triangle 128 x 256 blocks
   int splits;
   double* Kt;       // n x n, Kt[y*n + x] = K[x][y] for tile(x) >= tile(y); FP64 so
                     // the split-K sum does not depend on the atomics' order
   int* err;
 };
 
-constexpr int G2_STAGE = 4 * TILE_A_BYTES;
-constexpr int G2_STAGES = 3;
+constexpr int G2_BN = 256;
+constexpr int G2_STAGE = 6 * TILE_A_BYTES;           // A hi, lo (128 rows) + B hi, lo (256 rows)
+constexpr int G2_STAGES = 2;
 constexpr int G2_SMEM = G2_STAGES * G2_STAGE + 1024 + 1024;
-
 constexpr int G2_EPI = 2;                            // epilogue warps per TMEM lane quadrant
 constexpr int G2_THREADS = 64 + 4 * 32 * G2_EPI;     // TMA warp, MMA warp, epilogue warps
-constexpr int G2_COLS = BM / G2_EPI;                 // accumulator columns per epilogue warp
+constexpr int G2_COLS = G2_BN / G2_EPI;              // accumulator columns per epilogue warp
+static_assert(G2_SMEM <= SMEM_LIMIT, "GEMM2 ring exceeds shared memory");
 
-// Accumulation groups of ACC_GROUP k-blocks go to alternating TMEM buffers;
-// the epilogue adds each group's FP32 partial to FP64 totals in registers and
-// adds the totals to Kt once at the end.
+__host__ __device__ inline int g2_block_count(int nt) {
+  int c = 0;
+  for (int tx = 0; tx < nt; ++tx) c += tx / 2 + 1;
+  return c;
+}
+__device__ inline void g2_block(int b, int nt, int& tx, int& cp) {
+  tx = 0;
+  for (; tx < nt; ++tx) {
+    const int c = tx / 2 + 1;
+    if (b < c) break;
+    b -= c;
+  }
+  cp = b;
+}
+
+// Accumulation groups of ACC_GROUP k-blocks go to alternating TMEM buffers of
+// 256 columns; the epilogue adds each group's FP32 partial to FP32 totals in
+// registers (round-to-nearest) and adds the totals to Kt once at the end.
 __global__ void __launch_bounds__(G2_THREADS, 1)
     k_gemm2(const __grid_constant__ CUtensorMap tXh, const __grid_constant__ CUtensorMap tXl, const G2Params P) {
   extern __shared__ uint8_t smem_raw[];
@@ -317,17 +337,12 @@ __global__ void __launch_bounds__(G2_THREADS, 1)
   uint64_t* drain = tempty + 2;
   uint32_t* tmem_slot = (uint32_t*)(drain + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // which lower-triangle tile and which slice of the inner index
-  const int tile = blockIdx.x % P.ntiles_u, split = blockIdx.x / P.ntiles_u;
-  int tx = 0, ty = 0;
-  {
-    int r = tile;
-    while (r > tx) {
-      r -= tx + 1;
-      ++tx;
-    }
-    ty = r;
-  }
+  // which block of the lower triangle and which slice of the inner index
+  const int blk = blockIdx.x % P.nblocks, split = blockIdx.x / P.nblocks;
+  int tx, cp;
+  g2_block(blk, P.ntile_n, tx, cp);
+  // the second column tile is used when it lies on or below the diagonal
+  const bool wide = 2 * cp + 1 <= tx;
   const int kb0 = (int)((long long)P.kblocks * split / P.splits);
   const int kb1 = (int)((long long)P.kblocks * (split + 1) / P.splits);
 
@@ -345,7 +360,7 @@ __global__ void __launch_bounds__(G2_THREADS, 1)
     prefetch_tmap(&tXh);
     prefetch_tmap(&tXl);
   }
-  if (warp == 0) tmem_alloc(tmem_slot, 2 * BM);
+  if (warp == 0) tmem_alloc(tmem_slot, 2 * G2_BN);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -356,6 +371,7 @@ __global__ void __launch_bounds__(G2_THREADS, 1)
     if (lane == 0 && have_work) {
       int last_s = -1;
       uint32_t last_par = 0;
+      const uint32_t bytes = wide ? G2_STAGE : 4 * TILE_A_BYTES;
       for (int kb = kb0, it = 0; kb < kb1; ++kb, ++it) {
         const int s = it % G2_STAGES;
         const uint32_t j = it / G2_STAGES;
@@ -364,11 +380,16 @@ __global__ void __launch_bounds__(G2_THREADS, 1)
           break;
         }
         uint8_t* st = smem + s * G2_STAGE;
-        mbar_arrive_expect_tx(&full[s], G2_STAGE);
+        mbar_arrive_expect_tx(&full[s], bytes);
         tma_load_2d(st, &tXh, kb * BK, tx * BM, &full[s]);
         tma_load_2d(st + TILE_A_BYTES, &tXl, kb * BK, tx * BM, &full[s]);
-        tma_load_2d(st + 2 * TILE_A_BYTES, &tXh, kb * BK, ty * BM, &full[s]);
-        tma_load_2d(st + 3 * TILE_A_BYTES, &tXl, kb * BK, ty * BM, &full[s]);
+        // B: 256 (or 128) rows from column tile 2cp, hi then lo
+        tma_load_2d(st + 2 * TILE_A_BYTES, &tXh, kb * BK, 2 * cp * BM, &full[s]);
+        tma_load_2d(st + 4 * TILE_A_BYTES, &tXl, kb * BK, 2 * cp * BM, &full[s]);
+        if (wide) {
+          tma_load_2d(st + 3 * TILE_A_BYTES, &tXh, kb * BK, (2 * cp + 1) * BM, &full[s]);
+          tma_load_2d(st + 5 * TILE_A_BYTES, &tXl, kb * BK, (2 * cp + 1) * BM, &full[s]);
+        }
         last_s = s;
         last_par = j & 1;
       }
@@ -376,7 +397,7 @@ __global__ void __launch_bounds__(G2_THREADS, 1)
     }
   } else if (warp == 1) {
     if (lane == 0 && have_work) {
-      constexpr uint32_t idesc = idesc_bf16_f32(BM, BM);
+      const uint32_t idesc = wide ? idesc_bf16_f32(BM, G2_BN) : idesc_bf16_f32(BM, BM);
       bool ok = true;
       int it = 0, gt = 0;
       for (int kg = kb0; kg < kb1 && ok; kg += ACC_GROUP, ++gt) {
@@ -386,7 +407,7 @@ __global__ void __launch_bounds__(G2_THREADS, 1)
           break;
         }
         tc_fence_after();
-        const uint32_t d = tmem + b * BM;
+        const uint32_t d = tmem + b * G2_BN;
         const int kend = min(kg + ACC_GROUP, kb1);
         for (int kb = kg; kb < kend; ++kb, ++it) {
           const int s = it % G2_STAGES;
@@ -403,7 +424,7 @@ __global__ void __launch_bounds__(G2_THREADS, 1)
             const uint64_t ah = sdesc_kmajor_sw128(st + k * 32);
             const uint64_t al = sdesc_kmajor_sw128(st + TILE_A_BYTES + k * 32);
             const uint64_t bh = sdesc_kmajor_sw128(st + 2 * TILE_A_BYTES + k * 32);
-            const uint64_t bl = sdesc_kmajor_sw128(st + 3 * TILE_A_BYTES + k * 32);
+            const uint64_t bl = sdesc_kmajor_sw128(st + 4 * TILE_A_BYTES + k * 32);
             umma_bf16(d, ah, bh, idesc, (kb > kg || k > 0) ? 1u : 0u);
             umma_bf16(d, ah, bl, idesc, 1u);
             umma_bf16(d, al, bh, idesc, 1u);
@@ -418,9 +439,9 @@ __global__ void __launch_bounds__(G2_THREADS, 1)
   } else if (have_work) {  // warp w: TMEM lanes 32*(w%4).., columns [G2_COLS*part, +G2_COLS)
     const int q = warp & 3, part = (warp - 2) >> 2;
     const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) + part * G2_COLS;
-    double acc[G2_COLS];
+    float acc[G2_COLS];
 #pragma unroll
-    for (int e = 0; e < G2_COLS; ++e) acc[e] = 0.0;
+    for (int e = 0; e < G2_COLS; ++e) acc[e] = 0.0f;
     bool ok = true;
     for (int kg = kb0, gt = 0; kg < kb1; kg += ACC_GROUP, ++gt) {
       const int b = gt & 1;
@@ -430,24 +451,26 @@ __global__ void __launch_bounds__(G2_THREADS, 1)
         break;
       }
       tc_fence_after();
+      if (part == 0 || wide) {
 #pragma unroll
-      for (int c = 0; c < G2_COLS / 16; ++c) {
-        float v[16];
-        tmem_ld16(tbase + b * BM + c * 16, v);
-        tmem_ld_wait();
+        for (int c = 0; c < G2_COLS / 16; ++c) {
+          float v[16];
+          tmem_ld16(tbase + b * G2_BN + c * 16, v);
+          tmem_ld_wait();
 #pragma unroll
-        for (int e = 0; e < 16; ++e) acc[c * 16 + e] += (double)v[e];
+          for (int e = 0; e < 16; ++e) acc[c * 16 + e] += v[e];
+        }
       }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&tempty[b]);
     }
     const int x = tx * BM + 32 * q + lane;
-    if (ok && x < P.n) {
+    if (ok && x < P.n && (part == 0 || wide)) {
 #pragma unroll
       for (int e = 0; e < G2_COLS; ++e) {
-        const int y = ty * BM + part * G2_COLS + e;
-        if (y < P.n) atomicAdd(P.Kt + (size_t)y * P.n + x, acc[e]);
+        const int y = 2 * cp * BM + part * G2_COLS + e;
+        if (y < P.n) atomicAdd(P.Kt + (size_t)y * P.n + x, (double)acc[e]);
       }
     }
   }
@@ -455,7 +478,7 @@ __global__ void __launch_bounds__(G2_THREADS, 1)
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    tmem_dealloc(tmem, 2 * BM);
+    tmem_dealloc(tmem, 2 * G2_BN);
   }
 }
 
@@ -676,18 +699,7 @@ int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double
   cudaError_t st = dispatch_g1(NP, m.maps, P1, std::min(nsm, P1.ntiles), s);
   if (st != cudaSuccess) return check_cuda(e, st, "gemm1 launch");
   stage_mark(e, 1, s);
-  G2Params P2{};
-  P2.n = n;
-  P2.kblocks = (naux * NP) / BK;
-  P2.ntile_n = (n + BM - 1) / BM;
-  P2.ntiles_u = P2.ntile_n * (P2.ntile_n + 1) / 2;
-  P2.splits = std::max(1, std::min(nsm / P2.ntiles_u, P2.kblocks));
-  P2.Kt = m.Kt.p;
-  P2.err = m.err.p;
-  st = cudaFuncSetAttribute(k_gemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, G2_SMEM);
-  if (st != cudaSuccess) return check_cuda(e, st, "gemm2 attribute");
-  k_gemm2<<<P2.ntiles_u * P2.splits, G2_THREADS, G2_SMEM, s>>>(m.maps[4], m.maps[5], P2);
-  st = cudaGetLastError();
+  st = launch_gemm2(m.maps[4], m.maps[5], n, (naux * NP) / BK, m.Kt.p, m.err.p, nsm, s);
   if (st != cudaSuccess) return check_cuda(e, st, "gemm2 launch");
   stage_mark(e, 2, s);
   const int kchunk = (naux + 15) / 16;   // 16 K ranges per row x
@@ -735,20 +747,21 @@ cudaError_t launch_split_C(int n, int nocc, int NP, int ld, const double* C, __n
   return cudaGetLastError();
 }
 
-// Kt (+)= X X^T over the lower-triangle 128 x 128 tiles of the n rows of X
-// (tensor maps tXh, tXl over rows of `kblocks` * 64 BF16), split-K over the SMs.
+// Kt (+)= X X^T over the lower-triangle 128 x 256 blocks of the n rows of X
+// (tensor maps tXh, tXl over rows of `kblocks` * 64 BF16, boxes of 64 x 128),
+// split-K over the SMs.
 cudaError_t launch_gemm2(const CUtensorMap& tXh, const CUtensorMap& tXl, int n, int kblocks, double* Kt, int* err,
                          int nsm, cudaStream_t s) {
   G2Params P2{};
   P2.n = n;
   P2.kblocks = kblocks;
   P2.ntile_n = (n + BM - 1) / BM;
-  P2.ntiles_u = P2.ntile_n * (P2.ntile_n + 1) / 2;
+  P2.nblocks = g2_block_count(P2.ntile_n);
   // splits so that the CTA count is close to a whole number of waves
   int best = 1;
   double best_eff = 0.0;
-  for (int sp = 1; sp <= 16 && sp <= kblocks; ++sp) {
-    const int ctas = P2.ntiles_u * sp;
+  for (int sp = 1; sp <= 64 && sp <= kblocks; ++sp) {
+    const int ctas = P2.nblocks * sp;
     const double waves = std::ceil((double)ctas / nsm);
     const double eff = (double)ctas / (waves * nsm);
     if (eff > best_eff + 1e-9) {
@@ -762,7 +775,7 @@ cudaError_t launch_gemm2(const CUtensorMap& tXh, const CUtensorMap& tXl, int n, 
   P2.err = err;
   cudaError_t st = cudaFuncSetAttribute(k_gemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, G2_SMEM);
   if (st != cudaSuccess) return st;
-  k_gemm2<<<P2.ntiles_u * P2.splits, G2_THREADS, G2_SMEM, s>>>(tXh, tXl, P2);
+  k_gemm2<<<P2.nblocks * P2.splits, G2_THREADS, G2_SMEM, s>>>(tXh, tXl, P2);
   return cudaGetLastError();
 }
 
