@@ -113,6 +113,18 @@ int jk_direct_uhf_device(jk_engine* e, const double* dDa, const double* dDb, dou
 int jk_direct_noalloc(jk_engine* e, const double* dD, double precision, double multiplier, double* dJ,
                       double* dK, void* stream);
 
+/* Share the direct builds and the four-index gradient over nranks processes:
+ * every later jk_direct*, jk_direct_uhf* and jk_grad_rhf call on this engine
+ * evaluates only the bra shell pairs rank, rank + nranks, ... of every pair
+ * class (the Schwarz-sorted class lists interleave large and small pairs, so
+ * the shares carry nearly equal work) and returns this rank's partial J, K or
+ * gradient; the sum over ranks (one all-reduce of J and K, or of the 3 natom
+ * gradient) is the whole.  The one-body and nuclear-repulsion gradient terms
+ * go to rank 0 only.  The SCF driver and the SOAD guess always build the
+ * whole.  Default rank 0 of 1.  The loops split are those of
+ * src/fockbuild.cpp:88-158 and src/rhfgrad.cpp:454-590 (serial in molecular2). */
+int jk_direct_set_partition(jk_engine* e, int rank, int nranks);
+
 /* Number of shell quartets the last direct build (jk_direct, jk_direct_device
  * or jk_direct_noalloc) evaluated; -1 before the first build. */
 long long jk_last_quartets(const jk_engine* e);

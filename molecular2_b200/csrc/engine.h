@@ -98,6 +98,7 @@ struct MixedState {
   int NP_cap = 0;                    // NP the scratch below was allocated for
   DevBuf<__nv_bfloat16> Bh, Bl;      // [x][K][y], ld = ldb
   DevBuf<__nv_bfloat16> Ch, Cl;      // [i][y] (NP x ldb)
+  DevBuf<float> Cx;                  // [x][i] (n x NP), C for the gamma contraction
   DevBuf<__nv_bfloat16> Xh, Xl;      // [x][K][i] (n x naux*NP)
   DevBuf<double> Kt;                 // n x n partial K (lower-triangle tiles)
   DevBuf<int> err;                   // pipeline error word
@@ -121,6 +122,7 @@ struct TiledDF {
   int NPX_cap = 0;                   // NPX the mixed scratch was allocated for
   int waux_max = 0, oc_max = 0;      // caps on the aux block and the FP64 occupied slice (0: memory decides)
   DevBuf<__nv_bfloat16> Ch, Cl;      // [i][y], NPX x npad
+  DevBuf<float> Cx;                  // [x][i], npad x NPX, C for the gamma contraction
   DevBuf<__nv_bfloat16> Xh, Xl;      // [x][K_local][i], npad x waux x NPX
   DevBuf<double> Kt;                 // n x n lower-tile K
   DevBuf<int> err;
@@ -134,6 +136,11 @@ struct jk_engine {
   cudaStream_t stream = nullptr;
   // side streams of the per-class kernel launches (direct J/K, gradient):
   // forked from and joined back to the call's stream with events
+  // bra-pair partition of the public direct J/K and gradient calls (rank r of
+  // nranks takes the pairs r, r + nranks, ... of every class); internal callers
+  // (SCF, SOAD) always build the whole
+  int part_rank = 0, part_size = 1;
+  bool part_active = false;
   static constexpr int NCLS_STREAMS = 8;
   cudaStream_t cls_stream[NCLS_STREAMS] = {};
   cudaEvent_t cls_fork = nullptr, cls_join[NCLS_STREAMS] = {};
@@ -207,6 +214,9 @@ void stage_mark(jk_engine* e, int k, cudaStream_t s);
 int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double* dK, cudaStream_t s);
 int df_mixed_error(jk_engine* e);
 bool make_map(CUtensorMap* m, const void* base, uint64_t cols, uint64_t rows, uint32_t box_cols, uint32_t box_rows);
+// Cx[x][i] = C[x][i] in FP32 for x < n, i < nocc, zero in the padding (rows
+// up to nrow, columns up to NP)
+cudaError_t launch_rows_C(int n, int nocc, int NP, int nrow, const double* C, float* Cx, cudaStream_t s);
 cudaError_t launch_split_C(int n, int nocc, int NP, int ld, const double* C, __nv_bfloat16* Ch, __nv_bfloat16* Cl,
                            cudaStream_t s);
 cudaError_t launch_gemm2(const CUtensorMap& tXh, const CUtensorMap& tXl, int n, int kblocks, double* Kt, int* err,
@@ -226,6 +236,21 @@ void launch_final_to_cart(const jk_engine* e, const double* Dfinal, double* Dcar
 void launch_cart_to_final_sym(const jk_engine* e, const double* Xcart, double scale, double* Xfinal, cudaStream_t s);
 void launch_shell_norms(const jk_engine* e, const double* Dfinal, double* Dnorm, double* Dmax, cudaStream_t s);
 void launch_add(const double* a, const double* b, double* c, size_t n, cudaStream_t s);  // c = a + b
+
+// Makes the engine's bra-pair partition apply for the lifetime of the object
+// (the public direct J/K and gradient entry points).
+struct PartitionScope {
+  jk_engine* e;
+  explicit PartitionScope(jk_engine* e_) : e(e_) { e->part_active = true; }
+  ~PartitionScope() { e->part_active = false; }
+};
+// First bra pair and stride of this rank's share, and how many of the npair
+// pairs of a class that is.
+inline void bra_share(const jk_engine* e, int npair, int& bra0, int& step, int& count) {
+  bra0 = e->part_active ? e->part_rank : 0;
+  step = e->part_active ? e->part_size : 1;
+  count = npair > bra0 ? (npair - bra0 + step - 1) / step : 0;
+}
 
 // Per-class launches on side streams: ClassStreams cs(e, s) makes every side
 // stream wait for the work already queued on s; cs.next(cost) picks the side

@@ -44,11 +44,15 @@ __global__ void k_scale_K(int n, const double* __restrict__ K, const double* __r
 
 // kets per 64-thread block: one per thread, halved for classes with few bra
 // pairs so that their blocks still spread over the SMs
-static void launch_grad2e(int A, int B, const Grad2eParams& Pin, int nbra, int nket, cudaStream_t s) {
+static void launch_grad2e(const jk_engine* e, int A, int B, const Grad2eParams& Pin, int nbra, int nket,
+                          cudaStream_t s) {
   Grad2eParams P = Pin;
+  int nb = 0;
+  bra_share(e, nbra, P.bra0, P.bra_step, nb);
+  if (nb == 0) return;
   P.kchunk = 64;
-  if ((long long)nbra * ((nket + 63) / 64) < 4 * 148) P.kchunk = 32;
-  dim3 grid(nbra, (nket + P.kchunk - 1) / P.kchunk);
+  if ((long long)nb * ((nket + 63) / 64) < 4 * 148) P.kchunk = 32;
+  dim3 grid(nb, (nket + P.kchunk - 1) / P.kchunk);
   if (A <= 2)
     launch_grad2e_bra_s(A, B, P, grid, s);
   else if (A == 3)
@@ -161,10 +165,12 @@ int grad_rhf_device(jk_engine* e, const double* dD, const double* dW, double pre
     Q.bra_sig = sig[it.A].p;
     Q.ket_sig = sig[it.B].p;
     Q.same_class = (it.A == it.B);
-    launch_grad2e(it.A, it.B, Q, e->pcls[it.A].npair, e->pcls[it.B].npair, cs.next(it.cost));
+    launch_grad2e(e, it.A, it.B, Q, e->pcls[it.A].npair, e->pcls[it.B].npair, cs.next(it.cost));
   }
   cs.join();
-  for (int k = 0; k < NPAIRCLASS; ++k) {
+  // one-body terms: whole on the first rank of a partition, none on the others
+  const bool with_1e = !(e->part_active && e->part_rank != 0);
+  for (int k = 0; k < NPAIRCLASS && with_1e; ++k) {
     if (!e->pcls[k].npair) continue;
     Grad1eParams Q{};
     Q.pairs = view(e->pcls[k]);
@@ -207,7 +213,12 @@ extern "C" int jk_grad_rhf(jk_engine* e, const double* D, const double* W, doubl
   if (st == cudaSuccess) st = cudaMemcpyAsync(dD.p, D, sizeof(double) * n * n, cudaMemcpyHostToDevice, e->stream);
   if (st == cudaSuccess) st = cudaMemcpyAsync(dW.p, W, sizeof(double) * n * n, cudaMemcpyHostToDevice, e->stream);
   if (st != cudaSuccess) return check_cuda(e, st, "jk_grad_rhf upload");
-  int rc = grad_rhf_device(e, dD.p, dW.p, precision, g2.p, g1.p, e->stream, true);
+  const bool first = e->part_rank == 0;
+  int rc;
+  {
+    PartitionScope part(e);
+    rc = grad_rhf_device(e, dD.p, dW.p, precision, g2.p, g1.p, e->stream, true);
+  }
   if (rc) return rc;
   std::vector<double> h2(3 * na), h1(3 * na);
   st = cudaMemcpy(h2.data(), g2.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost);
@@ -215,6 +226,7 @@ extern "C" int jk_grad_rhf(jk_engine* e, const double* D, const double* W, doubl
   if (st != cudaSuccess) return check_cuda(e, st, "jk_grad_rhf download");
   std::vector<double> gn;
   nuclear_repulsion_grad(e, gn);
+  if (!first) std::fill(gn.begin(), gn.end(), 0.0);  // the first rank adds it
   for (int i = 0; i < 3 * na; ++i) grad[i] = h1[i] + h2[i] + gn[i];
   if (grad2e)
     for (int i = 0; i < 3 * na; ++i) grad2e[i] = h2[i];

@@ -69,13 +69,14 @@ struct Grad2eParams {
   const double* boys;
   double* grad;        // 3 * natom
   int kchunk;
+  int bra0, bra_step;        // block x handles bra pair bra0 + x * bra_step (a rank's share of the class)
 };
 
 template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(64) k_grad2e(const Grad2eParams P) {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   constexpr int N4 = NA * NB * NC * ND;
-  const int bra = blockIdx.x;
+  const int bra = P.bra0 + blockIdx.x * P.bra_step;
   if (!P.bra_sig[bra]) return;
   const int a = P.bra.sa[bra], b = P.bra.sb[bra];
   const double Qab = P.bra.Q[bra];

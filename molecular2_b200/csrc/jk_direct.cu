@@ -195,10 +195,14 @@ static void launch_classes(jk_engine* e, cudaStream_t s, Launch&& launch) {
   cs.join();
 }
 
-static void launch_jk(int A, int B, const JKParams& Pin, int nbra, int nket_max, cudaStream_t s, int nden = 1) {
+static void launch_jk(const jk_engine* e, int A, int B, const JKParams& Pin, int nbra, int nket_max, cudaStream_t s,
+                      int nden = 1) {
   JKParams P = Pin;
-  P.kchunk = ket_chunk(nbra, nket_max);
-  dim3 grid(nbra, (nket_max + P.kchunk - 1) / P.kchunk);
+  int nb = 0;
+  bra_share(e, nbra, P.bra0, P.bra_step, nb);
+  if (nb == 0) return;
+  P.kchunk = ket_chunk(nb, nket_max);
+  dim3 grid(nb, (nket_max + P.kchunk - 1) / P.kchunk);
   if (A <= 2)
     launch_jk_bra_s(A, B, nden, P, grid, s);
   else if (A == 3)
@@ -253,7 +257,7 @@ int direct_jk_device(jk_engine* e, const double* dD, double precision, double mu
     Q.ket = view(e->pcls[B]);
     Q.same_class = (A == B);
     Q.work = e->class_work.p + 3 * (A * NPAIRCLASS + B);
-    launch_jk(A, B, Q, e->pcls[A].npair, e->pcls[B].npair, cs);
+    launch_jk(e, A, B, Q, e->pcls[A].npair, e->pcls[B].npair, cs);
   });
   // J = 1/4 (J + J^T) mult, K = 1/2 * 1/4 (K + K^T) mult  (src/fockbuild.cpp:146-149, 161-162)
   launch_cart_to_final_sym(e, e->Jcart.p, 0.25 * mult, dJ, s);
@@ -310,7 +314,7 @@ int direct_jk_uhf_device(jk_engine* e, const double* dDa, const double* dDb, dou
     Q.ket = view(e->pcls[B]);
     Q.same_class = (A == B);
     Q.work = e->class_work.p + 3 * (A * NPAIRCLASS + B);
-    launch_jk(A, B, Q, e->pcls[A].npair, e->pcls[B].npair, cs, 2);
+    launch_jk(e, A, B, Q, e->pcls[A].npair, e->pcls[B].npair, cs, 2);
   });
   launch_cart_to_final_sym(e, Jc2.p, 0.25 * mult, dJa, s);
   launch_cart_to_final_sym(e, Jc2.p + ncc, 0.25 * mult, dJb, s);
@@ -409,7 +413,7 @@ int direct_jk_noalloc(jk_engine* e, const double* dD, double precision, double m
     Q.bra = view(e->pcls[A]);
     Q.ket = view(e->pcls[B]);
     Q.same_class = (A == B);
-    launch_jk(A, B, Q, e->pcls[A].npair, e->pcls[B].npair, cs);
+    launch_jk(e, A, B, Q, e->pcls[A].npair, e->pcls[B].npair, cs);
   });
   launch_cart_to_final_sym(e, Jc, 0.25 * mult, dJ, s);
   launch_cart_to_final_sym(e, Kc, 0.125 * mult, dK, s);
@@ -426,6 +430,7 @@ int jk_direct_uhf_device(jk_engine* e, const double* dDa, const double* dDb, dou
                          double* dJa, double* dJb, double* dKa, double* dKb, void* stream) {
   if (!e || !dDa || !dDb || !dJa || !dJb || !dKa || !dKb) return JK_ERR_ARG;
   if (!(precision >= 0.0)) return set_error(e, JK_ERR_ARG, "jk_direct_uhf: precision must be >= 0");
+  PartitionScope part(e);
   return direct_jk_uhf_device(e, dDa, dDb, precision, multiplier, dJa, dJb, dKa, dKb,
                               stream ? (cudaStream_t)stream : e->stream);
 }
@@ -470,6 +475,7 @@ int jk_direct_noalloc(jk_engine* e, const double* dD, double precision, double m
   if (!e || !dD || !dJ || !dK) return JK_ERR_ARG;
   if (!(precision >= 0.0)) return set_error(e, JK_ERR_ARG, "jk_direct_noalloc: precision must be >= 0");
   cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+  PartitionScope part(e);
   return direct_jk_noalloc(e, dD, precision, multiplier, dJ, dK, s);
 }
 
@@ -478,7 +484,17 @@ int jk_direct_device(jk_engine* e, const double* dD, double precision, double mu
   if (!e || !dD || !dJ || !dK) return JK_ERR_ARG;
   if (!(precision >= 0.0)) return set_error(e, JK_ERR_ARG, "jk_direct: precision must be >= 0");
   cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+  PartitionScope part(e);
   return direct_jk_device(e, dD, precision, multiplier, dJ, dK, s);
+}
+
+int jk_direct_set_partition(jk_engine* e, int rank, int nranks) {
+  if (!e) return JK_ERR_ARG;
+  if (nranks < 1 || rank < 0 || rank >= nranks)
+    return set_error(e, JK_ERR_ARG, "jk_direct_set_partition: need 0 <= rank < nranks");
+  e->part_rank = rank;
+  e->part_size = nranks;
+  return JK_OK;
 }
 
 int jk_direct(jk_engine* e, const double* D, double precision, double multiplier, double* J, double* K) {

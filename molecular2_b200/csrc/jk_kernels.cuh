@@ -187,6 +187,7 @@ struct JKParams {
   unsigned long long* counter;
   unsigned long long* work;  // NULL or this class pair's [quartets, sum bra primitive pairs, sum primitive quartets]
   int kchunk;
+  int bra0, bra_step;        // block x handles bra pair bra0 + x * bra_step (a rank's share of the class)
 };
 
 // Pairs of a class are sorted by Schwarz bound Q descending and then, inside
@@ -225,7 +226,7 @@ template <int LA, int LB, int LC, int LD, int NDEN = 1>
 __global__ void __launch_bounds__(128) k_jk_direct(const JKParams P) {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   constexpr bool BIG = NA * NB * NC * ND > UNROLL_LIMIT;
-  const int bra = blockIdx.x;
+  const int bra = P.bra0 + blockIdx.x * P.bra_step;
   const int a = P.bra.sa[bra], b = P.bra.sb[bra];
   const double Qab = P.bra.Q[bra];
   const double Dmax = *P.Dmax;

@@ -42,6 +42,7 @@ SIGNATURES = {
     "jk_df_uhf": (_I, [_P, _P, _I, _P, _I, _I, _D, _P, _P, _P, _P]),
     "jk_df_uhf_device": (_I, [_P, _P, _I, _P, _I, _I, _D, _P, _P, _P, _P, _P]),
     "jk_last_quartets": (ctypes.c_longlong, [_P]),
+    "jk_direct_set_partition": (_I, [_P, _I, _I]),
     "jk_last_class_work": (_I, [_P, _P, _I, ctypes.POINTER(_I)]),
     "jk_eri3": (_I, [_P, _P]),
     "jk_eri2": (_I, [_P, _P]),
@@ -239,6 +240,12 @@ class IntegralEngine:
         e = ctypes.c_double(0.0)
         self._check(self.lib.jk_df_mp2(self.h, _p(C), _p(eps), C.shape[1], nocc, nfrozen, ctypes.byref(e)))
         return e.value
+
+    def set_direct_partition(self, rank, nranks):
+        """Later direct J/K builds and four-index gradients evaluate only this
+        rank's share of the bra shell pairs (rank, rank + nranks, ... of every
+        class) and return partial results that sum over ranks to the whole."""
+        self._check(self.lib.jk_direct_set_partition(self.h, int(rank), int(nranks)))
 
     def wait_selftest(self, polls=1024):
         """Bounded-wait check: (gave up on a barrier nothing completes,

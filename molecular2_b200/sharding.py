@@ -1,5 +1,6 @@
-"""Density-fitted J/K sharded over ranks (one process per GPU).
+"""J/K builds and gradients sharded over ranks (one process per GPU).
 
+Density fitting:
 The fitted three-index tensor B[x][K][y] = sum_P (xy|P) (L^-T)_PK splits
 along the fitted index K with no coupling between slices:
 
@@ -56,3 +57,49 @@ def df_jk_sharded(engine, dC, nocc, dJ, dK, prec_mode=0, stream=None, group=None
     with torch.cuda.stream(s):
         allreduce_jk(dJ, dK, group)
     return dJ, dK
+
+
+# ---------------------------------------------------------------- direct J/K and gradient
+# The unique shell quartets of the direct build are (bra pair, ket pair) with
+# the bra pairs of every angular class sorted by their Schwarz bound.  Rank r
+# of R takes the bra pairs r, r + R, r + 2R, ... of every class
+# (IntegralEngine.set_direct_partition), so each rank gets pairs from the whole
+# range of bounds and nearly the same work; J, K (and the gradient) are sums
+# over quartets, so one all-reduce completes them (the loops of
+# src/fockbuild.cpp:88-158 and src/rhfgrad.cpp:454-590 split over ranks).
+
+def interleaved_share(n, rank, world):
+    """Indices rank, rank + world, ... below n: a rank's share of a sorted list."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("need 0 <= rank < world")
+    return list(range(rank, n, world))
+
+
+def direct_jk_sharded(engine, D, precision=1e-12, multiplier=1.0, group=None):
+    """One sharded direct J/K build from a host density D (numpy): this rank's
+    partial J and K, then the all-reduce; returns the whole (J, K) as numpy
+    arrays on every rank.  The process group may be NCCL (the partials are
+    moved to this rank's GPU) or gloo (CPU)."""
+    import numpy as np
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    engine.set_direct_partition(rank, world)
+    J, K = engine.jk_direct(D, precision, multiplier)
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    tJ = torch.from_numpy(np.ascontiguousarray(J)).to(dev)
+    tK = torch.from_numpy(np.ascontiguousarray(K)).to(dev)
+    allreduce_jk(tJ, tK, group)
+    return tJ.cpu().numpy(), tK.cpu().numpy()
+
+
+def gradient_sharded(engine, D, W, group=None):
+    """Sharded four-index RHF gradient: this rank's share of the two-electron
+    quartets (rank 0 adds the one-body and nuclear terms), then one all-reduce
+    of the 3 natom vector; returns the whole gradient (natom x 3)."""
+    import numpy as np
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    engine.set_direct_partition(rank, world)
+    g, _ = engine.compute_forces(D, W)
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.from_numpy(np.ascontiguousarray(g)).to(dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.cpu().numpy()

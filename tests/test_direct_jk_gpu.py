@@ -73,3 +73,46 @@ def test_direct_jk_multiplier_and_zero_density():
     J2, K2 = eng.jk_direct(D, 1e-12, -0.5)
     np.testing.assert_allclose(J2, -0.5 * J1, atol=1e-14)
     np.testing.assert_allclose(K2, -0.5 * K1, atol=1e-14)
+
+
+def test_direct_partition_sums_to_full_build():
+    """Bra-pair partition of the direct build and the four-index gradient
+    (jk_direct_set_partition): three ranks' partial J, K, UHF J/K and
+    gradients, computed on one GPU one after another, sum to the whole, the
+    quartet counts add up, and the interleaved shares carry nearly equal work."""
+    mol = geometry.water_cluster(8, 7.0, seed=8)
+    b = BasisSet(mol, "cc-pvdz")
+    eng = _engine(b)
+    D = _rand_density(b.nbf, 3)
+    Db = _rand_density(b.nbf, 4)
+    J, K = eng.jk_direct(D, 1e-12)
+    q_full = eng.last_quartets()
+    Ja, Jb, Ka, Kb = eng.jk_direct_uhf(D, Db, 1e-12)
+    W = 0.3 * D
+    g_full, _ = eng.compute_forces(D, W)
+    R = 3
+    sJ, sK, sq = np.zeros_like(J), np.zeros_like(K), []
+    su = [np.zeros_like(J) for _ in range(4)]
+    sg = np.zeros_like(g_full)
+    for r in range(R):
+        eng.set_direct_partition(r, R)
+        j, k = eng.jk_direct(D, 1e-12)
+        sJ += j
+        sK += k
+        sq.append(eng.last_quartets())
+        for acc, part in zip(su, eng.jk_direct_uhf(D, Db, 1e-12)):
+            acc += part
+        g, _ = eng.compute_forces(D, W)
+        sg += g
+    eng.set_direct_partition(0, 1)
+    scale = max(np.max(np.abs(J)), np.max(np.abs(K)))
+    assert np.max(np.abs(sJ - J)) < 1e-11 * scale and np.max(np.abs(sK - K)) < 1e-11 * scale
+    for acc, full in zip(su, (Ja, Jb, Ka, Kb)):
+        assert np.max(np.abs(acc - full)) < 1e-11 * scale
+    assert np.max(np.abs(sg - g_full)) < 1e-10
+    assert sum(sq) == q_full
+    print(f"quartets per rank {sq} of {q_full}")
+    assert max(sq) < 1.1 * q_full / R
+    # the SCF and the whole-build calls are not partitioned
+    J2, K2 = eng.jk_direct(D, 1e-12)
+    assert np.max(np.abs(J2 - J)) < 1e-12 * scale

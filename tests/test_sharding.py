@@ -56,3 +56,72 @@ def test_sharded_jk_two_gloo_ranks(tmp_path):
     J1, K1 = oracle.df_jk(B, C, nthreads=1)
     assert np.max(np.abs(J2 - J1)) < 1e-12
     assert np.max(np.abs(K2 - K1)) < 1e-12
+
+
+# ---------------------------------------------------------------- direct J/K and gradient
+class _OracleDirectEngine:
+    """Duck-typed stand-in for IntegralEngine on CPU: its partial direct build
+    is the oracle's restatement of Fock::formJKdirect over the shell rows s1 of
+    this rank's interleaved share (the GPU engine shares the bra pairs of every
+    class the same way; its partial builds are checked on the GPU in
+    test_direct_jk_gpu.py)."""
+
+    def __init__(self, basis):
+        import oracle
+        self.basis, self.Q = basis, oracle.schwarz(basis)
+        self.rank, self.world = 0, 1
+
+    def set_direct_partition(self, rank, world):
+        self.rank, self.world = rank, world
+
+    def jk_direct(self, D, precision=1e-12, multiplier=1.0):
+        import oracle
+        from molecular2_b200.sharding import interleaved_share
+        n = self.basis.nbf
+        J, K = np.zeros((n, n)), np.zeros((n, n))
+        for s1 in interleaved_share(self.Q.shape[0], self.rank, self.world):
+            j, k, _ = oracle.jk_direct_rows(self.basis, D, self.Q, precision, s1, s1 + 1)
+            J += j
+            K += k
+        return multiplier * J, multiplier * K
+
+
+def _direct_worker(rank, world, port, D, out):
+    from molecular2_b200 import geometry
+    from molecular2_b200.basis import BasisSet
+    from molecular2_b200.sharding import direct_jk_sharded
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        eng = _OracleDirectEngine(BasisSet(geometry.water(), "cc-pvdz"))
+        J, K = direct_jk_sharded(eng, D)
+        if rank == 0:
+            np.save(out, np.stack([J, K]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_interleaved_share_cover():
+    from molecular2_b200.sharding import interleaved_share
+    for n, world in [(10, 3), (7, 7), (3, 5), (100, 8)]:
+        got = sorted(i for r in range(world) for i in interleaved_share(n, r, world))
+        assert got == list(range(n))
+    with pytest.raises(ValueError):
+        interleaved_share(5, 2, 2)
+
+
+def test_direct_jk_sharded_two_gloo_ranks(tmp_path):
+    from molecular2_b200 import geometry
+    from molecular2_b200.basis import BasisSet
+    basis = BasisSet(geometry.water(), "cc-pvdz")
+    rng = np.random.default_rng(2)
+    C = np.linalg.qr(rng.normal(size=(basis.nbf, 5)))[0]
+    D = np.asfortranarray(2.0 * C @ C.T)
+    out = str(tmp_path / "djk.npy")
+    port = 29700 + os.getpid() % 1000
+    mp.start_processes(_direct_worker, args=(2, port, D, out), nprocs=2, start_method="spawn")
+    J2, K2 = np.load(out)
+    J1, K1 = _OracleDirectEngine(basis).jk_direct(D)
+    assert np.max(np.abs(J2 - J1)) < 1e-12
+    assert np.max(np.abs(K2 - K1)) < 1e-12
+    assert np.max(np.abs(J1)) > 1e-3
