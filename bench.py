@@ -329,10 +329,25 @@ def measure_direct(local):
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / nb
     q = eng.last_quartets()
+    work = eng.last_class_work()
     eng.close()
+    # FP64 work of the build from the frozen per-class table (flops per bra
+    # primitive pair, per primitive quartet, per quartet of digestion)
+    table = json.load(open(os.path.join(ROOT, "molecular2_b200", "data", "flop_table.json")))["table"]
+    flops = 0.0
+    for A in range(6):
+        for B in range(A + 1):
+            t = table[f"{A},{B}"]
+            nq, wb, wq = (float(x) for x in work[A, B])
+            flops += t["bra"] * wb + t["quartet"] * wq + t["digest"] * nq
+    fp64_peak = 40.0   # TFLOP/s, nominal B200 FP64 (no measured FP64 figure is available)
+    roof = {"kernel": "k_jk_direct (all classes)", "bound": "fp64", "flops_per_build": flops,
+            "achieved_tflops": flops / (ms * 1e-3) / 1e12, "peak_tflops": fp64_peak, "peak_source": "nominal",
+            "frac": flops / (ms * 1e-3) / 1e12 / fp64_peak,
+            "work_model": "molecular2_b200/data/flop_table.json x jk_last_class_work counts"}
     return {"workload": f"C20H42 RHF/6-311G** FP64 integral-direct J/K build (n={n}), seed 20, SOAD-guess density, "
                         "Schwarz x density screen 1e-12",
-            "ms_per_build": ms, "quartets": q, "quartets_per_s": q / (ms * 1e-3)}
+            "ms_per_build": ms, "quartets": q, "quartets_per_s": q / (ms * 1e-3), "roofline": roof}
 
 
 def measure_water16(local):

@@ -45,7 +45,7 @@ struct G1Params {
   int nocc;
   int n, naux;
   int ntiles;
-  const double* C;  // n x nocc column-major
+  const float* Cx;  // [x][i] n x NP, C in FP32 (zero padded)
   __nv_bfloat16* Xhi;  // [m][NP]
   __nv_bfloat16* Xlo;
   double* gamma;
@@ -105,11 +105,17 @@ __device__ __forceinline__ bool g1_epilogue_tile(uint32_t tbase, int& gt, int ng
   }
   if (NV == 0 || m >= P.M) return true;
   const int x = m / P.naux, K = m - x * P.naux;
-  const double* Cx = P.C + x;
+  // gamma_K += sum_i X[x][K][i] C[x][i]: the row of C as 16-byte vectors
+  const float4* c4 = reinterpret_cast<const float4*>(P.Cx + (size_t)x * NP + C0 * 16);
   double g4[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-  for (int i = 0; i < NV; ++i)
-    if (C0 * 16 + i < P.nocc) g4[i & 3] += (double)v[i] * __ldg(Cx + (size_t)(C0 * 16 + i) * P.n);
+  for (int i = 0; i < NV / 4; ++i) {
+    const float4 c = __ldg(c4 + i);
+    g4[0] += (double)v[4 * i] * c.x;
+    g4[1] += (double)v[4 * i + 1] * c.y;
+    g4[2] += (double)v[4 * i + 2] * c.z;
+    g4[3] += (double)v[4 * i + 3] * c.w;
+  }
   atomicAdd(P.gamma + K, (g4[0] + g4[1]) + (g4[2] + g4[3]));
   uint4* oh = reinterpret_cast<uint4*>(P.Xhi + (size_t)m * NP + C0 * 16);
   uint4* ol = reinterpret_cast<uint4*>(P.Xlo + (size_t)m * NP + C0 * 16);
@@ -649,6 +655,7 @@ int df_mixed_prepare(jk_engine* e, int nocc) {
     // reuse it with tensor maps for their own row length
     if (NP > m.NP_cap) {
       st = m.Ch.alloc((size_t)NP * ldb);
+      if (st == cudaSuccess) st = m.Cx.alloc((size_t)n * NP);
       if (st == cudaSuccess) st = m.Cl.alloc((size_t)NP * ldb);
       if (st == cudaSuccess) st = m.Xh.alloc((size_t)n * naux * NP);
       if (st == cudaSuccess) st = m.Xl.alloc((size_t)n * naux * NP);
@@ -680,6 +687,7 @@ int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device);
   stage_mark(e, 0, s);
   k_split_C<<<dim3((ldb + 127) / 128, NP), 128, 0, s>>>(n, nocc, NP, ldb, dC, m.Ch.p, m.Cl.p);
+  launch_rows_C(n, nocc, NP, n, dC, m.Cx.p, s);
   cudaMemsetAsync(d.gamma.p, 0, sizeof(double) * naux, s);
   cudaMemsetAsync(m.Kt.p, 0, sizeof(double) * n * n, s);
   cudaMemsetAsync(dJ, 0, sizeof(double) * n * n, s);
@@ -690,7 +698,7 @@ int df_mixed_device(jk_engine* e, const double* dC, int nocc, double* dJ, double
   P1.n = n;
   P1.naux = naux;
   P1.ntiles = (P1.M + BM - 1) / BM;
-  P1.C = dC;
+  P1.Cx = m.Cx.p;
   P1.Xhi = m.Xh.p;
   P1.Xlo = m.Xl.p;
   P1.gamma = d.gamma.p;
@@ -741,6 +749,19 @@ int df_mixed_error(jk_engine* e) {
 }
 
 // ---------------------------------------------------------------- shared with the tiled path
+__global__ void k_rows_C(int n, int nocc, int NP, int nrow, const double* __restrict__ C, float* __restrict__ Cx) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)nrow * NP) return;
+  const int x = (int)(idx / NP), i = (int)(idx % NP);
+  Cx[idx] = (x < n && i < nocc) ? (float)C[x + (size_t)i * n] : 0.0f;
+}
+
+cudaError_t launch_rows_C(int n, int nocc, int NP, int nrow, const double* C, float* Cx, cudaStream_t s) {
+  const size_t tot = (size_t)nrow * NP;
+  k_rows_C<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(n, nocc, NP, nrow, C, Cx);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_split_C(int n, int nocc, int NP, int ld, const double* C, __nv_bfloat16* Ch, __nv_bfloat16* Cl,
                            cudaStream_t s) {
   k_split_C<<<dim3((ld + 127) / 128, NP), 128, 0, s>>>(n, nocc, NP, ld, C, Ch, Cl);

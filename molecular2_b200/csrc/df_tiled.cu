@@ -81,7 +81,7 @@ struct S1Params {
   int k0, wstride;   // first fitted function of the block; X row stride in K
   int nhalf, nitems;
   int nocc, n, NPX;
-  const double* C;   // n x nocc column-major
+  const float* Cx;   // [x][i] npad x NPX, C in FP32 (zero padded)
   __nv_bfloat16* Xh;  // [x][K_local][NPX]
   __nv_bfloat16* Xl;
   double* gamma;     // global fitted index
@@ -133,11 +133,17 @@ __device__ __forceinline__ bool s1_epilogue_item(uint32_t tbase, int& gt, int ng
     if (lane == 0) mbar_arrive(&tempty[b]);
   }
   const int i0 = h * SN + C0 * 16;
-  if (x < P.n) {
+  if (x < P.n) {  // gamma_K += sum_i X[x][K][i] C[x][i], the row of C as 16-byte vectors
+    const float4* c4 = reinterpret_cast<const float4*>(P.Cx + (size_t)x * P.NPX + i0);
     double g4[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int i = 0; i < NV; ++i)
-      if (i0 + i < P.nocc) g4[i & 3] += (double)v[i] * __ldg(P.C + x + (size_t)(i0 + i) * P.n);
+    for (int i = 0; i < NV / 4; ++i) {
+      const float4 c = __ldg(c4 + i);
+      g4[0] += (double)v[4 * i] * c.x;
+      g4[1] += (double)v[4 * i + 1] * c.y;
+      g4[2] += (double)v[4 * i + 2] * c.z;
+      g4[3] += (double)v[4 * i + 3] * c.w;
+    }
     atomicAdd(P.gamma + P.k0 + Kl, (g4[0] + g4[1]) + (g4[2] + g4[3]));
   }
   const size_t row = ((size_t)x * P.wstride + Kl) * P.NPX + i0;
@@ -631,6 +637,7 @@ static int tiled_mixed_prepare(jk_engine* e, int nocc) {
     T.Xh.reset();
     T.Xl.reset();
     st = T.Ch.alloc((size_t)NPX * T.npad);
+    if (st == cudaSuccess) st = T.Cx.alloc((size_t)NPX * T.npad);
     if (st == cudaSuccess) st = T.Cl.alloc((size_t)NPX * T.npad);
     if (st == cudaSuccess) st = T.Kt.alloc((size_t)n * n);
     if (st == cudaSuccess) st = T.err.alloc(1);
@@ -686,6 +693,7 @@ static int tiled_mixed(jk_engine* e, const double* dC, int nocc, double* dJ, dou
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e->device);
   stage_mark(e, 0, s);
   cudaError_t st = launch_split_C(n, nocc, T.NPX, T.npad, dC, T.Ch.p, T.Cl.p, s);
+  if (st == cudaSuccess) st = launch_rows_C(n, nocc, T.NPX, T.npad, dC, T.Cx.p, s);
   if (st != cudaSuccess) return check_cuda(e, st, "split C");
   cudaMemsetAsync(d.gamma.p, 0, sizeof(double) * naux, s);
   cudaMemsetAsync(T.Kt.p, 0, sizeof(double) * n * n, s);
@@ -717,7 +725,7 @@ static int tiled_mixed(jk_engine* e, const double* dC, int nocc, double* dJ, dou
     P.nocc = nocc;
     P.n = n;
     P.NPX = T.NPX;
-    P.C = dC;
+    P.Cx = T.Cx.p;
     P.Xh = T.Xh.p;
     P.Xl = T.Xl.p;
     P.gamma = d.gamma.p;
