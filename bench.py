@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the J/K engine on (H2O)64 / aug-cc-pVDZ + AVDZ-JKFIT.
 
-Workload (the north-star system): 64 rigid water monomers placed by seeded
+Workload: 64 rigid water monomers placed by seeded
 random rotation and translation in a 14 A cube (O-O >= 2.7 A), RHF with the
 aug-cc-pVDZ orbital basis (n = 2624) and the AVDZ-JKFIT fitting basis
 (naux = 9600), nocc = 320: the density-fitted J/K build molecular2 runs every
@@ -39,7 +39,7 @@ extrapolated linearly in naux.
 --precision fp64 times FP64 builds instead of mixed ones; --workload water16aug
 is the small case of the tiled kernels used for ncu captures.
 With --gpus N > 1 every rank runs its own replica of the workload (the
-north-star measurement is single-GPU).
+headline measurement is single-GPU).
 """
 import argparse
 import ctypes
