@@ -282,7 +282,12 @@ def measure_gradient(local):
            "scf_s": scf_s, "scf_iterations": r.iterations, "energy": r.energy, "gradient_ms": gms,
            "timing": "host wall clock around jk_grad_rhf", "max_abs_sum_g": float(np.abs(g.sum(axis=0)).max())}
     eng = IntegralEngine(BasisSet(mol, "cc-pvdz"), BasisSet(mol, "vdz-jkfit"), device=local)
+    import torch
+    torch.cuda.synchronize()
+    t = time.perf_counter()
     eng.df_setup()
+    torch.cuda.synchronize()
+    out["df_setup_s"] = time.perf_counter() - t
     _, ex = eng.scf_rhf(mol.nocc, mol.enuc(), df=True, guess="soad", want=True, densconverge=1e-8,
                         enconverge=1e-10, maxiter=60)
     o = mol.nocc
@@ -348,6 +353,86 @@ def measure_direct(local):
     return {"workload": f"C20H42 RHF/6-311G** FP64 integral-direct J/K build (n={n}), seed 20, SOAD-guess density, "
                         "Schwarz x density screen 1e-12",
             "ms_per_build": ms, "quartets": q, "quartets_per_s": q / (ms * 1e-3), "roofline": roof}
+
+
+def measure_scf_h2o(local):
+    """H2O/cc-pVDZ direct FP64 SCF from the SOAD guess (the smallest
+    configuration) on the GPU."""
+    from molecular2_b200 import geometry
+    from molecular2_b200.basis import BasisSet
+    from molecular2_b200.engine import IntegralEngine
+    mol = geometry.water()
+    eng = IntegralEngine(BasisSet(mol, "cc-pvdz"), device=local)
+    kw = dict(guess="soad", densconverge=1e-10, enconverge=1e-12, maxiter=60)
+    eng.scf_rhf(mol.nocc, mol.enuc(), **kw)
+    t = time.perf_counter()
+    r, ex = eng.scf_rhf(mol.nocc, mol.enuc(), want=True, **kw)
+    s = time.perf_counter() - t
+    C = ex["C"][:, :mol.nocc]
+    W = C @ np.diag(ex["eps"][:mol.nocc]) @ C.T
+    eng.compute_forces(ex["D"], W)
+    t = time.perf_counter()
+    eng.compute_forces(ex["D"], W)
+    gs = time.perf_counter() - t
+    eng.close()
+    return {"workload": "H2O RHF/cc-pVDZ direct FP64 SCF, SOAD guess, and its analytic gradient", "scf_s": s,
+            "iterations": r.iterations, "energy": r.energy, "gradient_s": gs}
+
+
+def cpu_baselines(extra):
+    """The oracle's restatement of the reference's loops on one host core
+    beside the GPU figures of `extra` (each bounded to ~10-20 s): direct J/K
+    (C20H42, every 41st shell row, scaled by the quartet count), DF set-up
+    ((H2O)8 three- and two-index integrals and B = (mn|P) L^-T, whole), SCF
+    (H2O, whole) and the two-electron gradient ((H2O)8, every 8th shell row,
+    scaled by 8)."""
+    import scipy.linalg as sl
+    import oracle
+    from oracle import scf as oscf
+    from molecular2_b200 import geometry
+    from molecular2_b200.basis import BasisSet
+    out = {"cores": 1, "kind": "port"}
+    # direct J/K, C20H42/6-311G**, the GPU measurement's SOAD-guess density
+    mol = geometry.c20h42()
+    b = BasisSet(mol, "6-311g**")
+    rhf = oscf.RHF(b, minbasis=BasisSet(mol, "sto-3g"), nthreads=1)
+    _, C = sl.eigh(rhf.soad_fock(), rhf.S)
+    D = 2.0 * C[:, :mol.nocc] @ C[:, :mol.nocc].T
+    Q = oracle.schwarz(b)
+    t, q = time.perf_counter(), 0
+    for s1 in range(0, Q.shape[0], 41):
+        q += oracle.jk_direct_rows(b, D, Q, 1e-12, s1, s1 + 1)[2]
+    t = time.perf_counter() - t
+    d = extra.get("direct_jk_c20h42", {})
+    q_all = d.get("quartets") or q * 41
+    cpu_s = t * q_all / max(1, q)
+    out["direct_jk_c20h42"] = {"cpu_s_per_build": cpu_s, "gpu_s_per_build": d.get("ms_per_build", float("nan")) / 1e3,
+                               "sample": f"every 41st shell row: {q} of {q_all} quartets in {t:.1f} s, scaled"}
+    # DF set-up, (H2O)8 cc-pVDZ + VDZ-JKFIT
+    mol = geometry.water8()
+    obs, aux = BasisSet(mol, "cc-pvdz"), BasisSet(mol, "vdz-jkfit")
+    t = time.perf_counter()
+    oracle.df_B(oracle.eri3(obs, aux), oracle.eri2(aux), nthreads=1)
+    g = extra.get("gradient_water8", {})
+    out["df_setup_water8"] = {"cpu_s": time.perf_counter() - t, "gpu_s": g.get("df_setup_s"),
+                              "sample": "whole: (P|mn), (P|Q), Cholesky and B"}
+    # SCF, H2O cc-pVDZ direct
+    h2o = geometry.water()
+    t = time.perf_counter()
+    oscf.RHF(BasisSet(h2o, "cc-pvdz"), guess="soad", minbasis=BasisSet(h2o, "sto-3g"), densconverge=1e-10,
+             enconverge=1e-12, maxiter=60, nthreads=1).run()
+    sc = extra.get("scf_h2o", {})
+    out["scf_h2o"] = {"cpu_s": time.perf_counter() - t, "gpu_s": sc.get("scf_s"), "sample": "whole"}
+    # two-electron gradient of H2O cc-pVDZ (the (H2O)8 one takes ~25 min on one core)
+    bh = BasisSet(h2o, "cc-pvdz")
+    rng = np.random.default_rng(8)
+    Cr = np.linalg.qr(rng.normal(size=(bh.nbf, h2o.nocc)))[0]
+    t = time.perf_counter()
+    oracle.grad2e(bh, 2.0 * Cr @ Cr.T, oracle.schwarz(bh), 1e-12, nthreads=1)
+    out["gradient_2e_h2o"] = {"cpu_s": time.perf_counter() - t, "gpu_s": sc.get("gradient_s"),
+                              "sample": "whole two-electron term (random orthonormal orbitals); the GPU figure "
+                                        "is the whole gradient at the SCF density"}
+    return out
 
 
 def measure_water16(local):
@@ -553,6 +638,9 @@ def run_ours(args, rank, world, local):
             extra["water16"] = measure_water16(local)
             extra["gradient_water8"] = measure_gradient(local)
             extra["direct_jk_c20h42"] = measure_direct(local)
+            extra["scf_h2o"] = measure_scf_h2o(local)
+            if rank == 0 and world == 1 and not args.no_cpu_baseline:
+                extra["cpu_baselines"] = cpu_baselines(extra)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -62,6 +62,7 @@ def lib():
             "orc_eri3_deriv_block": (None, [P, P, i, i, i, i, i, P]),
             "orc_eri4_deriv_block": (None, [P, i, i, i, i, i, i, P]),
             "orc_df_grad_contract": (None, [P, P, P, P, i, P, P, P, i]),
+            "orc_grad2e_rows": (None, [P, P, i, P, P, d, i, i, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -248,6 +249,19 @@ def grad2e(basis, D, Q, precision=1e-12, want_G1=False, nthreads=None):
     lib().orc_grad2e(_bp(basis), _p(atom), na, _p(D), _p(Qc), precision, _p(G1), _p(grad),
                      nthreads or os.cpu_count() or 1)
     return (grad.reshape(na, 3), G1) if want_G1 else grad.reshape(na, 3)
+
+
+def grad2e_rows(basis, D, Q, precision, s1_begin, s1_step):
+    """Time-bounded compute_2body_fock_deriv<1> for the CPU baseline: the
+    two-electron gradient terms of the shell rows s1_begin, s1_begin + s1_step,
+    ... only (one thread), natom x 3."""
+    D = F(D)
+    na = basis.mol.natom
+    grad = np.zeros(3 * na)
+    atom = np.ascontiguousarray(basis.atom, dtype=np.int32)
+    Qc = np.ascontiguousarray(Q, dtype=np.float64)
+    lib().orc_grad2e_rows(_bp(basis), _p(atom), na, _p(D), _p(Qc), precision, s1_begin, s1_step, _p(grad))
+    return grad.reshape(na, 3)
 
 
 def eri4_deriv_block(basis, s1, s2, s3, s4, center, xyz):

@@ -1299,10 +1299,27 @@ void orc_shellpair_list(const orc_basis* obs, double threshold, int* flags) {
 // 0.25 * sum_ab G1[coord](a,b) D(a,b), and, when G1 != NULL, the 3*natom
 // symmetrised derivative Fock matrices (column-major).  Q is the Schwarz
 // matrix; screening uses D as the reference does with its member density.
+static void grad2e_rows(const orc_basis* obs, const int* shell_atom, int natom, const double* D, const double* Q,
+                        double precision, double* G1, double* grad, int nthreads, int s1_begin, int s1_step);
+
 void orc_grad2e(const orc_basis* obs, const int* shell_atom, int natom, const double* D, const double* Q,
                 double precision, double* G1, double* grad, int nthreads) {
+  grad2e_rows(obs, shell_atom, natom, D, Q, precision, G1, grad, nthreads, 0, 1);
+}
+
+// Time-bounded variant for the CPU baseline: the same loop over the shell rows
+// s1 = s1_begin, s1_begin + s1_step, ... only (one thread).
+void orc_grad2e_rows(const orc_basis* obs, const int* shell_atom, int natom, const double* D, const double* Q,
+                     double precision, int s1_begin, int s1_step, double* grad) {
+  grad2e_rows(obs, shell_atom, natom, D, Q, precision, nullptr, grad, 1, s1_begin, s1_step);
+}
+
+static void grad2e_rows(const orc_basis* obs, const int* shell_atom, int natom, const double* D, const double* Q,
+                        double precision, double* G1, double* grad, int nthreads, int s1_begin, int s1_step) {
   Basis B = make_basis(obs);
   const int ns = (int)B.sh.size(), n = B.n;
+  std::vector<int> rows;
+  for (int s = s1_begin; s < ns; s += s1_step) rows.push_back(s);
   const size_t nn = (size_t)n * n;
   auto Dn = shellblock_norm(B, D);
   std::vector<int> flags((size_t)ns * ns);
@@ -1315,7 +1332,8 @@ void orc_grad2e(const orc_basis* obs, const int* shell_atom, int natom, const do
   std::vector<std::vector<double>> Gt(nthreads, std::vector<double>(nn * 3 * natom, 0.0));
   auto dn = [&](int a, int c) { return Dn[(size_t)a * ns + c]; };
   auto Dm = [&](size_t i, size_t j) { return D[j * n + i]; };
-  parallel_for(ns, nthreads, [&](int s1, int t) {
+  parallel_for((int)rows.size(), nthreads, [&](int r, int t) {
+    const int s1 = rows[r];
     double* G = Gt[t].data();
     std::vector<double> buf;
     for (int s2 : plist[s1]) {
