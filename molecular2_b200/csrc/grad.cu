@@ -52,7 +52,7 @@ static void launch_grad2e(const jk_engine* e, int A, int B, const Grad2eParams& 
   if (nb == 0) return;
   P.kchunk = 64;
   if ((long long)nb * ((nket + 63) / 64) < 4 * 148) P.kchunk = 32;
-  dim3 grid(nb, (nket + P.kchunk - 1) / P.kchunk);
+  dim3 grid(nb, (nket + P.kchunk - 1) / P.kchunk, 6);  // z: the six shifted classes
   if (A <= 2)
     launch_grad2e_bra_s(A, B, P, grid, s);
   else if (A == 3)

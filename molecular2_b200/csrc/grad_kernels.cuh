@@ -72,10 +72,17 @@ struct Grad2eParams {
   int bra0, bra_step;        // block x handles bra pair bra0 + x * bra_step (a rank's share of the class)
 };
 
+// One shifted class per block layer: blockIdx.z = 0, 1 (centre a raised,
+// lowered), 2, 3 (b), 4, 5 (c); the derivative with respect to centre d follows
+// from translational invariance (minus the sum of the other three).  Splitting
+// the six shifted quartets over blocks shortens each thread's serial work six
+// times, which is what bounds the d classes of small molecules.
 template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(64) k_grad2e(const Grad2eParams P) {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   constexpr int N4 = NA * NB * NC * ND;
+  const int sh = blockIdx.z, centre = sh >> 1;
+  if ((sh == 1 && LA == 0) || (sh == 3 && LB == 0) || (sh == 5 && LC == 0)) return;
   const int bra = P.bra0 + blockIdx.x * P.bra_step;
   if (!P.bra_sig[bra]) return;
   const int a = P.bra.sa[bra], b = P.bra.sb[bra];
@@ -93,6 +100,7 @@ __global__ void __launch_bounds__(64) k_grad2e(const Grad2eParams P) {
   const int bp0 = P.bra.prim_off[bra], bnp = P.bra.nprim[bra];
   const int nc = P.nc;
   const double* __restrict__ Dc = P.Dc;
+  double gbra[3] = {0, 0, 0};  // this thread's share for the bra centre (centre 0 or 1: one atom per block)
 
   for (int kl = start + threadIdx.x; kl < end; kl += blockDim.x) {
     if (!P.ket_sig[kl]) continue;
@@ -125,51 +133,62 @@ __global__ void __launch_bounds__(64) k_grad2e(const Grad2eParams P) {
           }
         }
       }
-    double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0}, gC[3] = {0, 0, 0};
-    {
+    double g[3] = {0, 0, 0};
+    if (sh == 0) {
       double I[ncart(LA + 1) * NB * NC * ND];
       quartet_cart<LA + 1, LB, LC, LD>(P.pp2a, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.pp, kp0, knp, Cx, Cy, Cz, Ex, Ey,
                                        Ez, P.boys, I);
-      contract_shift<LA, LB, LC, LD, 0, 1>(I, Wt, gA);
-    }
-    if constexpr (LA > 0) {
-      double I[ncart(LA - 1) * NB * NC * ND];
-      quartet_cart<LA - 1, LB, LC, LD>(P.pp, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.pp, kp0, knp, Cx, Cy, Cz, Ex, Ey, Ez,
-                                       P.boys, I);
-      contract_shift<LA, LB, LC, LD, 0, -1>(I, Wt, gA);
-    }
-    {
+      contract_shift<LA, LB, LC, LD, 0, 1>(I, Wt, g);
+    } else if (sh == 1) {
+      if constexpr (LA > 0) {
+        double I[ncart(LA - 1) * NB * NC * ND];
+        quartet_cart<LA - 1, LB, LC, LD>(P.pp, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.pp, kp0, knp, Cx, Cy, Cz, Ex, Ey,
+                                         Ez, P.boys, I);
+        contract_shift<LA, LB, LC, LD, 0, -1>(I, Wt, g);
+      }
+    } else if (sh == 2) {
       double I[NA * ncart(LB + 1) * NC * ND];
       quartet_cart<LA, LB + 1, LC, LD>(P.pp2b, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.pp, kp0, knp, Cx, Cy, Cz, Ex, Ey,
                                        Ez, P.boys, I);
-      contract_shift<LA, LB, LC, LD, 1, 1>(I, Wt, gB);
-    }
-    if constexpr (LB > 0) {
-      double I[NA * ncart(LB - 1) * NC * ND];
-      quartet_cart<LA, LB - 1, LC, LD>(P.pp, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.pp, kp0, knp, Cx, Cy, Cz, Ex, Ey, Ez,
-                                       P.boys, I);
-      contract_shift<LA, LB, LC, LD, 1, -1>(I, Wt, gB);
-    }
-    {
+      contract_shift<LA, LB, LC, LD, 1, 1>(I, Wt, g);
+    } else if (sh == 3) {
+      if constexpr (LB > 0) {
+        double I[NA * ncart(LB - 1) * NC * ND];
+        quartet_cart<LA, LB - 1, LC, LD>(P.pp, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.pp, kp0, knp, Cx, Cy, Cz, Ex, Ey,
+                                         Ez, P.boys, I);
+        contract_shift<LA, LB, LC, LD, 1, -1>(I, Wt, g);
+      }
+    } else if (sh == 4) {
       double I[NA * NB * ncart(LC + 1) * ND];
       quartet_cart<LA, LB, LC + 1, LD>(P.pp, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.pp2a, kp0, knp, Cx, Cy, Cz, Ex, Ey,
                                        Ez, P.boys, I);
-      contract_shift<LA, LB, LC, LD, 2, 1>(I, Wt, gC);
+      contract_shift<LA, LB, LC, LD, 2, 1>(I, Wt, g);
+    } else {
+      if constexpr (LC > 0) {
+        double I[NA * NB * ncart(LC - 1) * ND];
+        quartet_cart<LA, LB, LC - 1, LD>(P.pp, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.pp, kp0, knp, Cx, Cy, Cz, Ex, Ey,
+                                         Ez, P.boys, I);
+        contract_shift<LA, LB, LC, LD, 2, -1>(I, Wt, g);
+      }
     }
-    if constexpr (LC > 0) {
-      double I[NA * NB * ncart(LC - 1) * ND];
-      quartet_cart<LA, LB, LC - 1, LD>(P.pp, bp0, bnp, Ax, Ay, Az, Bx, By, Bz, P.pp, kp0, knp, Cx, Cy, Cz, Ex, Ey, Ez,
-                                       P.boys, I);
-      contract_shift<LA, LB, LC, LD, 2, -1>(I, Wt, gC);
-    }
-    const int at[4] = {P.atom[a], P.atom[b], P.atom[c], P.atom[d]};
+    const int atd = P.atom[d];
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
-      const double gD = -(gA[x] + gB[x] + gC[x]);
-      atomicAdd(P.grad + 3 * at[0] + x, deg * gA[x]);
-      atomicAdd(P.grad + 3 * at[1] + x, deg * gB[x]);
-      atomicAdd(P.grad + 3 * at[2] + x, deg * gC[x]);
-      atomicAdd(P.grad + 3 * at[3] + x, deg * gD);
+      const double v = deg * g[x];
+      if (centre < 2)
+        gbra[x] += v;
+      else
+        atomicAdd(P.grad + 3 * P.atom[c] + x, v);
+      atomicAdd(P.grad + 3 * atd + x, -v);  // d: minus the derivative of the shifted centre
+    }
+  }
+  if (centre < 2) {  // the bra centre's atom is the same for the whole block: one atomic per warp
+    const int at = P.atom[centre == 0 ? a : b];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      double v = gbra[x];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(P.grad + 3 * at + x, v);
     }
   }
 }
