@@ -363,7 +363,7 @@ def measure_scf_h2o(local):
     from molecular2_b200.engine import IntegralEngine
     mol = geometry.water()
     eng = IntegralEngine(BasisSet(mol, "cc-pvdz"), device=local)
-    kw = dict(guess="soad", densconverge=1e-10, enconverge=1e-12, maxiter=60)
+    kw = dict(guess="soad", densconverge=1e-8, enconverge=1e-10, maxiter=60)
     eng.scf_rhf(mol.nocc, mol.enuc(), **kw)
     t = time.perf_counter()
     r, ex = eng.scf_rhf(mol.nocc, mol.enuc(), want=True, **kw)
@@ -419,8 +419,8 @@ def cpu_baselines(extra):
     # SCF, H2O cc-pVDZ direct
     h2o = geometry.water()
     t = time.perf_counter()
-    oscf.RHF(BasisSet(h2o, "cc-pvdz"), guess="soad", minbasis=BasisSet(h2o, "sto-3g"), densconverge=1e-10,
-             enconverge=1e-12, maxiter=60, nthreads=1).run()
+    oscf.RHF(BasisSet(h2o, "cc-pvdz"), guess="soad", minbasis=BasisSet(h2o, "sto-3g"), densconverge=1e-8,
+             enconverge=1e-10, maxiter=60, nthreads=1).run()
     sc = extra.get("scf_h2o", {})
     out["scf_h2o"] = {"cpu_s": time.perf_counter() - t, "gpu_s": sc.get("scf_s"), "sample": "whole"}
     # two-electron gradient of H2O cc-pVDZ (the (H2O)8 one takes ~25 min on one core)
