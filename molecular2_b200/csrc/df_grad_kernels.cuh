@@ -74,73 +74,89 @@ struct Grad3Params {
   double* grad;           // 3 * natom
 };
 
+// One shifted class per block layer: blockIdx.z = 0, 1 (orbital centre m
+// raised, lowered), 2, 3 (n); the fitting centre's derivative is minus their
+// sum (translational invariance).  All threads of a block share the fitting
+// shell, so its atom's term is reduced over the warp first.
 template <int LP, int LM, int LN>
 __global__ void __launch_bounds__(64) k_grad3(const Grad3Params P) {
   constexpr int NP = ncart(LP), NM = ncart(LM), NN = ncart(LN);
   constexpr int N3 = NP * NM * NN;
-  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  const int sh = blockIdx.z;
+  if ((sh == 1 && LM == 0) || (sh == 3 && LN == 0)) return;
   const int is = blockIdx.y;
-  if (ip >= P.pairs.npair || is >= P.naux_shells) return;
+  if (is >= P.naux_shells) return;
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
   const int sP = P.aux_shells[is];
-  const int m = P.pairs.sa[ip], n = P.pairs.sb[ip];
-  // weights of this block, final basis -> Cartesian
-  const int pure[3] = {P.aux_pure[sP], P.obs_pure[m], P.obs_pure[n]};
-  const int ls[3] = {LP, LM, LN};
-  int dims[3] = {pure[0] ? 2 * LP + 1 : NP, pure[1] ? 2 * LM + 1 : NM, pure[2] ? 2 * LN + 1 : NN};
-  double w0[N3], w1[N3];
-  const int f0 = P.aux_foff[sP], m0 = P.obs_foff[m], n0 = P.obs_foff[n];
-  for (int a = 0; a < dims[0]; ++a)
-    for (int x = 0; x < dims[1]; ++x)
-      for (int y = 0; y < dims[2]; ++y)
-        w0[(a * dims[1] + x) * dims[2] + y] = P.W3[((size_t)(f0 - P.w3_f0 + a) * P.n + n0 + y) * P.n + m0 + x];
-  double* cur = w0;
-  double* nxt = w1;
-  for (int k = 0; k < 3; ++k)
-    if (pure[k]) {
-      sph_index_adj(cur, nxt, k, dims, ls[k], k == 0 ? P.sph_aux : P.sph_obs);
-      dims[k] = ncart(ls[k]);
-      double* sw = cur;
-      cur = nxt;
-      nxt = sw;
+  double g[3] = {0, 0, 0};
+  if (ip < P.pairs.npair) {
+    const int m = P.pairs.sa[ip], n = P.pairs.sb[ip];
+    // weights of this block, final basis -> Cartesian
+    const int pure[3] = {P.aux_pure[sP], P.obs_pure[m], P.obs_pure[n]};
+    const int ls[3] = {LP, LM, LN};
+    int dims[3] = {pure[0] ? 2 * LP + 1 : NP, pure[1] ? 2 * LM + 1 : NM, pure[2] ? 2 * LN + 1 : NN};
+    double w0[N3], w1[N3];
+    const int f0 = P.aux_foff[sP], m0 = P.obs_foff[m], n0 = P.obs_foff[n];
+    for (int a = 0; a < dims[0]; ++a)
+      for (int x = 0; x < dims[1]; ++x)
+        for (int y = 0; y < dims[2]; ++y)
+          w0[(a * dims[1] + x) * dims[2] + y] = P.W3[((size_t)(f0 - P.w3_f0 + a) * P.n + n0 + y) * P.n + m0 + x];
+    double* cur = w0;
+    double* nxt = w1;
+    for (int k = 0; k < 3; ++k)
+      if (pure[k]) {
+        sph_index_adj(cur, nxt, k, dims, ls[k], k == 0 ? P.sph_aux : P.sph_obs);
+        dims[k] = ncart(ls[k]);
+        double* sw = cur;
+        cur = nxt;
+        nxt = sw;
+      }
+    const double* Wt = cur;  // [a][x][y] Cartesian, as a (LP, 0 | LM, LN) block
+    const double Px = P.ax[sP], Py = P.ay[sP], Pz = P.az[sP];
+    const double Ax = P.ox[m], Ay = P.oy[m], Az = P.oz[m], Bx = P.ox[n], By = P.oy[n], Bz = P.oz[n];
+    const int ap0 = P.aux_prim_off[sP], anp = P.aux_nprim[sP];
+    const int kp0 = P.pairs.prim_off[ip], knp = P.pairs.nprim[ip];
+    if (sh == 0) {
+      double I[NP * ncart(LM + 1) * NN];
+      quartet_cart_ool<LP, 0, LM + 1, LN>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp2a, kp0, knp, Ax, Ay, Az, Bx,
+                                          By, Bz, P.boys, I);
+      contract_shift<LP, 0, LM, LN, 2, 1>(I, Wt, g);
+    } else if (sh == 1) {
+      if constexpr (LM > 0) {
+        double I[NP * ncart(LM - 1) * NN];
+        quartet_cart_ool<LP, 0, LM - 1, LN>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp, kp0, knp, Ax, Ay, Az, Bx,
+                                            By, Bz, P.boys, I);
+        contract_shift<LP, 0, LM, LN, 2, -1>(I, Wt, g);
+      }
+    } else if (sh == 2) {
+      double I[NP * NM * ncart(LN + 1)];
+      quartet_cart_ool<LP, 0, LM, LN + 1>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp2b, kp0, knp, Ax, Ay, Az, Bx,
+                                          By, Bz, P.boys, I);
+      contract_shift<LP, 0, LM, LN, 3, 1>(I, Wt, g);
+    } else {
+      if constexpr (LN > 0) {
+        double I[NP * NM * ncart(LN - 1)];
+        quartet_cart_ool<LP, 0, LM, LN - 1>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp, kp0, knp, Ax, Ay, Az, Bx,
+                                            By, Bz, P.boys, I);
+        contract_shift<LP, 0, LM, LN, 3, -1>(I, Wt, g);
+      }
     }
-  const double* Wt = cur;  // [a][x][y] Cartesian, as a (LP, 0 | LM, LN) block
-  const double Px = P.ax[sP], Py = P.ay[sP], Pz = P.az[sP];
-  const double Ax = P.ox[m], Ay = P.oy[m], Az = P.oz[m], Bx = P.ox[n], By = P.oy[n], Bz = P.oz[n];
-  const int ap0 = P.aux_prim_off[sP], anp = P.aux_nprim[sP];
-  const int kp0 = P.pairs.prim_off[ip], knp = P.pairs.nprim[ip];
-  double gM[3] = {0, 0, 0}, gN[3] = {0, 0, 0};
-  {
-    double I[NP * ncart(LM + 1) * NN];
-    quartet_cart_ool<LP, 0, LM + 1, LN>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp2a, kp0, knp, Ax, Ay, Az, Bx,
-                                        By, Bz, P.boys, I);
-    contract_shift<LP, 0, LM, LN, 2, 1>(I, Wt, gM);
+    // the sum over ordered (m, n) counts an off-diagonal canonical pair twice
+    const double deg = (m == n) ? 1.0 : 2.0;
+    const int at = P.obs_atom[sh < 2 ? m : n];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      g[x] *= deg;
+      if (g[x] != 0.0) atomicAdd(P.grad + 3 * at + x, g[x]);
+    }
   }
-  if constexpr (LM > 0) {
-    double I[NP * ncart(LM - 1) * NN];
-    quartet_cart_ool<LP, 0, LM - 1, LN>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp, kp0, knp, Ax, Ay, Az, Bx, By,
-                                        Bz, P.boys, I);
-    contract_shift<LP, 0, LM, LN, 2, -1>(I, Wt, gM);
-  }
-  {
-    double I[NP * NM * ncart(LN + 1)];
-    quartet_cart_ool<LP, 0, LM, LN + 1>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp2b, kp0, knp, Ax, Ay, Az, Bx,
-                                        By, Bz, P.boys, I);
-    contract_shift<LP, 0, LM, LN, 3, 1>(I, Wt, gN);
-  }
-  if constexpr (LN > 0) {
-    double I[NP * NM * ncart(LN - 1)];
-    quartet_cart_ool<LP, 0, LM, LN - 1>(P.ap, ap0, anp, Px, Py, Pz, Px, Py, Pz, P.pp, kp0, knp, Ax, Ay, Az, Bx, By,
-                                        Bz, P.boys, I);
-    contract_shift<LP, 0, LM, LN, 3, -1>(I, Wt, gN);
-  }
-  // the sum over ordered (m, n) counts an off-diagonal canonical pair twice
-  const double deg = (m == n) ? 1.0 : 2.0;
-  const int am = P.obs_atom[m], an = P.obs_atom[n], aP = P.aux_atom[sP];
+  // the fitting centre: minus the orbital centres' terms, one atomic per warp
+  const int aP = P.aux_atom[sP];
 #pragma unroll
   for (int x = 0; x < 3; ++x) {
-    atomicAdd(P.grad + 3 * am + x, deg * gM[x]);
-    atomicAdd(P.grad + 3 * an + x, deg * gN[x]);
-    atomicAdd(P.grad + 3 * aP + x, -deg * (gM[x] + gN[x]));
+    double v = g[x];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(P.grad + 3 * aP + x, -v);
   }
 }
 

@@ -5,7 +5,7 @@
 
 namespace m2 {
 void launch_grad3_l2(int pc, const Grad3Params& P, cudaStream_t s) {
-  dim3 grid((P.pairs.npair + 63) / 64, P.naux_shells);
+  dim3 grid((P.pairs.npair + 63) / 64, P.naux_shells, 4);  // z: the four shifted classes
   if (pc == 0) k_grad3<2, 0, 0><<<grid, 64, 0, s>>>(P);
   if (pc == 1) k_grad3<2, 1, 0><<<grid, 64, 0, s>>>(P);
   if (pc == 2) k_grad3<2, 1, 1><<<grid, 64, 0, s>>>(P);
