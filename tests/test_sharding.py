@@ -125,3 +125,41 @@ def test_direct_jk_sharded_two_gloo_ranks(tmp_path):
     assert np.max(np.abs(J2 - J1)) < 1e-12
     assert np.max(np.abs(K2 - K1)) < 1e-12
     assert np.max(np.abs(J1)) > 1e-3
+
+
+class _SplitGradientEngine:
+    """Duck-typed engine whose partial gradient is the rank's share of a fixed
+    per-row decomposition of a known gradient (the GPU partition itself is
+    checked in test_direct_jk_gpu.py)."""
+
+    def __init__(self, parts):
+        self.parts = parts  # rows x natom x 3
+        self.rank, self.world = 0, 1
+
+    def set_direct_partition(self, rank, world):
+        self.rank, self.world = rank, world
+
+    def compute_forces(self, D, W):
+        from molecular2_b200.sharding import interleaved_share
+        g = sum(self.parts[i] for i in interleaved_share(len(self.parts), self.rank, self.world))
+        return g, g
+
+
+def _gradient_worker(rank, world, port, parts, out):
+    from molecular2_b200.sharding import gradient_sharded
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        g = gradient_sharded(_SplitGradientEngine(parts), None, None)
+        if rank == 0:
+            np.save(out, g)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gradient_sharded_three_gloo_ranks(tmp_path):
+    parts = np.random.default_rng(3).normal(size=(10, 4, 3))
+    out = str(tmp_path / "g.npy")
+    port = 29900 + os.getpid() % 100
+    mp.start_processes(_gradient_worker, args=(3, port, parts, out), nprocs=3, start_method="spawn")
+    assert np.max(np.abs(np.load(out) - parts.sum(axis=0))) < 1e-12
